@@ -1,0 +1,52 @@
+"""Builds libhrm.so (the runtime's C ABI and built-in specs) for sm_100a, in-tree.
+
+    python -m harmonize_b200.build [--force]
+
+nvcc cross-compiles without a GPU. The library lands next to this file so that it travels
+with the repository snapshot and is the one the tests and the bench load.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libhrm.so")
+SOURCES = [os.path.join(HERE, "csrc", "hrm_capi.cu")]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "-shared",
+              "-I", os.path.join(ROOT, "include")]
+
+
+def _deps():
+    out = list(SOURCES)
+    for d in (os.path.join(ROOT, "include"), os.path.join(HERE, "csrc")):
+        for dirpath, _, files in os.walk(d):
+            out += [os.path.join(dirpath, f) for f in files if f.endswith((".h", ".cuh", ".cu"))]
+    return out
+
+
+def needs_build():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(p) > t for p in _deps())
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and not needs_build():
+        return LIB
+    tmp = LIB + ".tmp"
+    cmd = ["nvcc"] + ARCH + NVCC_FLAGS + list(extra) + ["-o", tmp] + SOURCES + ["-lgomp"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,844 @@
+// async_program.h — AsyncProgram<Spec>: the persistent work-coalescing runtime.
+//
+// Source-level contract kept from harmonize/cpp/program/async.h:
+//  * the spec members and defaults (async.h:101-131), Instance(arena_links, DeviceState)
+//    with complete() / clear_flags() (async.h:302-384), init<P>/exec<P>;
+//  * prog.async<F>(args...), prog.sync<F>(args...), prog.load_fraction<F>() (NaN here, as in
+//    async.h:2902-2906), prog.halt_early(), prog.device / prog.group / prog.thread;
+//  * exec(cycles) runs at most `cycles` scheduling rounds per team, then leaves every
+//    pending promise in device memory so that the next exec resumes it (async.h:2625-2668);
+//  * completion: COMPLETION_FLAG is set only when every team found no work anywhere and
+//    every team's make_work returned false (async.h:2323-2393); a team that stops while
+//    make_work still wanted to run, or a halt_early() call, leaves the run incomplete.
+//
+// Internals (the B200 design, not a translation):
+//  * a "team" is one warp; a CTA holds TEAMS_PER_CTA teams. Each team owns, in shared
+//    memory, one ring per async function of RING_LINKS*32 promise slots, stored as
+//    structure-of-arrays 32-bit words (conflict-free for 32 consecutive slots).
+//  * prog.async<F>: the lanes active at the call site reserve slots with ONE shared-memory
+//    atomicAdd issued by the lowest lane (__activemask / popc rank / __shfl_sync), then each
+//    lane writes its own words. Promises of one function therefore land contiguously, and
+//    the scheduler evaluates them 32 at a time: every batch is warp-full while work lasts.
+//  * when a ring passes its high-water mark the team spills its oldest promises as whole
+//    links to the HBM arena: one atomicAdd claims all links needed, each lane stores one
+//    32-bit word per promise word (every store instruction covers 128 contiguous bytes),
+//    and one atomicAdd publishes all links to the function's lock-free ring.
+//  * an idle team fills from the arena the function closest to a full batch; teams count
+//    themselves busy/idle in one 64-bit word with a wake-up epoch, and quiescence is
+//    declared only when "all idle" and "all queues empty" hold across an unchanged epoch.
+//  * every wait is bounded (WAIT_TIMEOUT_FLAG), arena exhaustion is flagged
+//    (ARENA_EXHAUSTED_FLAG) and never silent.
+#ifndef HARMONIZE_B200_ASYNC_PROGRAM_H
+#define HARMONIZE_B200_ASYNC_PROGRAM_H
+
+#include "runtime_common.h"
+
+template <typename PROGRAM_SPEC>
+class AsyncProgram;
+
+namespace hrm_rt {
+template <typename PROG>
+__global__ void async_init_kernel(typename PROG::DeviceContext ctx);
+template <typename PROG>
+__global__ void async_prep_kernel(typename PROG::DeviceContext ctx, unsigned int total_teams);
+template <typename PROG>
+__global__ void __launch_bounds__(PROG::CTA_THREADS, PROG::MIN_CTAS_PER_SM)
+    async_exec_kernel(typename PROG::DeviceContext ctx, typename PROG::DeviceState device, unsigned int cycles);
+}  // namespace hrm_rt
+
+template <typename PROGRAM_SPEC>
+class AsyncProgram {
+   public:
+    typedef AsyncProgram<PROGRAM_SPEC> ProgramType;
+    typedef PROGRAM_SPEC Spec;
+
+    using AdrType = typename hrm_rt::spec_AdrType<PROGRAM_SPEC>::type;
+    using OpSet = typename hrm_rt::spec_OpSet<PROGRAM_SPEC>::type;
+    using DeviceState = typename hrm_rt::spec_DeviceState<PROGRAM_SPEC>::type;
+    using GroupState = typename hrm_rt::spec_GroupState<PROGRAM_SPEC>::type;
+    using ThreadState = typename hrm_rt::spec_ThreadState<PROGRAM_SPEC>::type;
+
+    typedef PromiseUnion<OpSet> PromiseUnionType;
+    typedef PromiseEnum<OpSet> PromiseEnumType;
+
+    template <typename TYPE>
+    struct Lookup {
+        typedef typename PromiseUnionType::template Lookup<TYPE>::type type;
+    };
+
+    static const size_t STASH_SIZE = hrm_rt::spec_STASH_SIZE<PROGRAM_SPEC>::value;
+    static const size_t FRAME_SIZE = hrm_rt::spec_FRAME_SIZE<PROGRAM_SPEC>::value;
+    static const size_t POOL_SIZE = hrm_rt::spec_POOL_SIZE<PROGRAM_SPEC>::value;
+    static const size_t STACK_SIZE = hrm_rt::spec_STACK_SIZE<PROGRAM_SPEC>::value;
+    static const size_t GROUP_SIZE = hrm_rt::spec_GROUP_SIZE<PROGRAM_SPEC>::value;
+    static const size_t WORK_GROUP_SIZE = GROUP_SIZE;
+    static_assert(GROUP_SIZE == 32, "work groups are 32-lane warps");
+
+    static const unsigned int RING_LINKS = (unsigned int)hrm_rt::spec_RING_LINKS<PROGRAM_SPEC>::value;
+    static const unsigned int RING = RING_LINKS * 32u;
+    static_assert(RING_LINKS >= 2 && (RING & (RING - 1)) == 0, "RING_LINKS must be a power of two >= 2");
+    static const unsigned int TEAMS_PER_CTA = (unsigned int)hrm_rt::spec_TEAMS_PER_CTA<PROGRAM_SPEC>::value;
+    static const unsigned int CTA_THREADS = TEAMS_PER_CTA * 32u;
+    static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
+
+    static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
+    static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
+    static const unsigned int COMPLETION_FLAG = hrm_rt::COMPLETION_FLAG;
+    static const unsigned int EARLY_HALT_FLAG = hrm_rt::EARLY_HALT_FLAG;
+
+    static const unsigned char FN_ID_COUNT = (unsigned char)PromiseUnionType::Info::COUNT;
+    static const unsigned int FN = FN_ID_COUNT;
+    static_assert(FN >= 1 && FN <= 16, "an operation set holds 1 to 16 async functions");
+
+    using Layout = OpLayout<OpSet>;
+    static const unsigned int TOTAL_WORDS = Layout::TOTAL_WORDS;
+    static const unsigned int LINK_WORDS = Layout::MAX_WORDS;  // words per promise in a link
+
+    // -----------------------------------------------------------------------------------
+    // Contexts (the names of async.h:181-262; contents are this runtime's).
+    // -----------------------------------------------------------------------------------
+    struct ThreadContext {
+        unsigned int thread_id;
+        unsigned int rand_state;
+    };
+
+    // One team's shared-memory stash: a ring of RING promise slots per function.
+    struct GroupContext {
+        unsigned int count[FN];    // promises held per function (may exceed RING briefly)
+        unsigned int bottom[FN];   // ring index of the oldest promise per function
+        unsigned int words[TOTAL_WORDS][RING];
+    };
+
+    struct DeviceContext {
+        typedef ProgramType ParentProgramType;
+        hrm_rt::RuntimeControl* ctl;
+        hrm_rt::RingSet rings;        // rings [0, FN) = per-function queues, ring FN = free links
+        unsigned int* link_words;     // arena: link l, word w, lane i at ((l*LINK_WORDS+w)*32+i)
+        unsigned int* link_meta;      // per link {next + 1, promise count}; used by barriers
+        unsigned long long* stats;    // hrm_rt::STAT_COUNT counters
+        unsigned int arena_links;
+    };
+
+    // -----------------------------------------------------------------------------------
+    // Host-side instance: owns the device memory of one program instance.
+    // -----------------------------------------------------------------------------------
+    struct Instance {
+        AdrType arena_size;
+        util::host::DevBuf<hrm_rt::RuntimeControl> control;
+        util::host::DevBuf<hrm_rt::RingHead> heads;
+        util::host::DevBuf<unsigned long long> slots;
+        util::host::DevBuf<unsigned int> link_words;
+        util::host::DevBuf<unsigned int> link_meta;
+        util::host::DevBuf<unsigned long long> stats;
+        unsigned int ring_capacity;
+        DeviceState device_state;
+        cudaStream_t stream = nullptr;
+
+        __host__ Instance(AdrType arsize, DeviceState ds)
+            : arena_size(arsize),
+              control((size_t)1),
+              heads((size_t)(FN + 1)),
+              slots((size_t)(FN + 1) * hrm_rt::next_pow2(arsize < 32 ? 32 : (unsigned long long)arsize)),
+              link_words((size_t)arsize * LINK_WORDS * 32u),
+              link_meta((size_t)arsize * 2u),
+              stats((size_t)hrm_rt::STAT_COUNT),
+              ring_capacity(hrm_rt::next_pow2(arsize < 32 ? 32 : (unsigned long long)arsize)),
+              device_state(ds) {
+            if ((unsigned long long)arsize >= (1ull << 27) - 2) {
+                throw std::runtime_error("AsyncProgram arena holds at most 2^27 - 2 links");
+            }
+            util::host::auto_throw(cudaMemset(control.data(), 0, sizeof(hrm_rt::RuntimeControl)));
+            util::host::auto_throw(cudaMemset(stats.data(), 0, sizeof(unsigned long long) * hrm_rt::STAT_COUNT));
+        }
+
+        __host__ DeviceContext to_context() {
+            DeviceContext c;
+            c.ctl = control.data();
+            c.rings.heads = heads.data();
+            c.rings.slots = slots.data();
+            c.rings.mask = ring_capacity - 1;
+            c.link_words = link_words.data();
+            c.link_meta = link_meta.data();
+            c.stats = stats.data();
+            c.arena_links = (unsigned int)arena_size;
+            return c;
+        }
+
+        __host__ unsigned int flags() {
+            unsigned int f = 0;
+            util::host::auto_throw(cudaMemcpy(&f, &control.data()->flags, sizeof(f), cudaMemcpyDeviceToHost));
+            return f;
+        }
+        // True once an exec found no work anywhere and make_work exhausted everywhere.
+        // Throws if the device raised an error flag, so that host loops end.
+        __host__ bool complete() {
+            unsigned int f = flags();
+            if (f & hrm_rt::ERROR_MASK) hrm_rt::throw_flags(f);
+            return (f & COMPLETION_FLAG) != 0;
+        }
+        __host__ void clear_flags() {
+            util::host::auto_throw(cudaMemset(&control.data()->flags, 0, sizeof(unsigned int)));
+        }
+        // Host-side view of the arena (the role of runtime_overview, async.h:2766-2883):
+        // out[0] = links handed out lazily (capped at the arena size), out[1] = links on the
+        // free ring, out[2 + f] = links queued for function f, out[2 + FN + r] = tail - head
+        // of ring r. A quiescent instance has out[0] == out[1] and every queue empty.
+        __host__ std::vector<unsigned int> overview() {
+            hrm_rt::RuntimeControl c;
+            std::vector<hrm_rt::RingHead> h(FN + 1);
+            util::host::auto_throw(cudaMemcpy(&c, control.data(), sizeof(c), cudaMemcpyDeviceToHost));
+            util::host::auto_throw(
+                cudaMemcpy(h.data(), heads.data(), sizeof(hrm_rt::RingHead) * (FN + 1), cudaMemcpyDeviceToHost));
+            std::vector<unsigned int> out;
+            out.push_back(c.bump < (unsigned int)arena_size ? c.bump : (unsigned int)arena_size);
+            out.push_back(h[FN].avail);
+            for (unsigned int f = 0; f < FN; f++) out.push_back(h[f].avail);
+            for (unsigned int r = 0; r <= FN; r++) out.push_back(h[r].tail - h[r].head);
+            return out;
+        }
+
+        __host__ std::vector<unsigned long long> read_stats() {
+            std::vector<unsigned long long> v(hrm_rt::STAT_COUNT);
+            util::host::auto_throw(cudaMemcpy(v.data(), stats.data(), sizeof(unsigned long long) * hrm_rt::STAT_COUNT,
+                                              cudaMemcpyDeviceToHost));
+            return v;
+        }
+    };
+
+    // -----------------------------------------------------------------------------------
+    // The program object handed to eval / make_work: references to the contexts.
+    // -----------------------------------------------------------------------------------
+    DeviceContext& _dev_ctx;
+    GroupContext& _grp_ctx;
+    ThreadContext& _thd_ctx;
+    DeviceState& device;
+    GroupState& group;
+    ThreadState& thread;
+
+    __device__ AsyncProgram(DeviceContext& d_c, GroupContext& g_c, ThreadContext& t_c, DeviceState& d,
+                            GroupState& g, ThreadState& t)
+        : _dev_ctx(d_c), _grp_ctx(g_c), _thd_ctx(t_c), device(d), group(g), thread(t) {}
+
+    // ===================================================================================
+    // Public device API used by specs.
+    // ===================================================================================
+    template <typename TYPE, typename... ARGS>
+    __device__ __forceinline__ void async(ARGS... args) {
+        push_promise<TYPE>(Promise<TYPE>(args...));
+    }
+    template <typename TYPE>
+    __device__ __forceinline__ void async_call(Promise<TYPE> promise) {
+        push_promise<TYPE>(promise);
+    }
+    // Runtime-discriminant form (used by barriers): lanes are grouped by discriminant
+    // with __match_any_sync and each group is pushed as one coalesced call.
+    __device__ void async_call(PromiseEnumType promise) { push_enum<0>(promise.disc, promise.data); }
+    __device__ void async_call(OpDisc disc, int, PromiseUnionType& promise) { push_enum<0>(disc, promise); }
+
+    template <typename TYPE, typename... ARGS>
+    __device__ __forceinline__ void sync(ARGS... args) {
+        Promise<TYPE>(args...)(*this);
+    }
+    template <typename TYPE>
+    __device__ __forceinline__ void sync_call(Promise<TYPE> promise) {
+        promise(*this);
+    }
+    template <typename TYPE>
+    __device__ float load_fraction() {
+        return NAN;
+    }
+    __device__ void halt_early() { atomicOr(&_dev_ctx.ctl->flags, EARLY_HALT_FLAG); }
+
+    // ===================================================================================
+    // Promise placement.
+    // ===================================================================================
+    template <typename TYPE>
+    __host__ __device__ static constexpr unsigned int disc_of() {
+        static_assert(OpUnionLookup<TYPE, OpSet>::CONTAINED, "async function is not in the spec's OpSet");
+        return OpUnionLookup<TYPE, OpSet>::DISC;
+    }
+
+    // Allocates `n` links for this lane (n <= 32, called by one lane). Returns how many
+    // were obtained; link j goes to *first + j for bump links, or is popped from the free ring.
+    // The lane-cooperative variant below is used instead wherever the whole warp is present.
+    __device__ unsigned int alloc_links_coop(unsigned int n, unsigned int j, unsigned int mask, unsigned int& link) {
+        // Lazy bump allocation first, then the free-link ring.
+        const unsigned int leader = __ffs(mask) - 1;
+        hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
+        unsigned int base = 0, from_bump = 0;
+        if (j == 0) {
+            unsigned int cur = hrm_rt::ld_relaxed(&ctl->bump);
+            if (cur < _dev_ctx.arena_links) {
+                base = atomicAdd(&ctl->bump, n);
+                if (base < _dev_ctx.arena_links) {
+                    from_bump = min(n, _dev_ctx.arena_links - base);
+                }
+            }
+        }
+        base = __shfl_sync(mask, base, leader);
+        from_bump = __shfl_sync(mask, from_bump, leader);
+        unsigned int need = n - from_bump;
+        unsigned int got_free = 0, pos = 0;
+        if (need > 0) {
+            if (j == 0) {
+                // Links on the free ring may be in the middle of being returned: retry a
+                // bounded number of times before reporting the arena as exhausted.
+                for (unsigned int attempt = 0; attempt < 64u; attempt++) {
+                    got_free = hrm_rt::ring_reserve(_dev_ctx.rings, FN, need, pos);
+                    if (got_free > 0) break;
+                    __nanosleep(256);
+                }
+            }
+            got_free = __shfl_sync(mask, got_free, leader);
+            pos = __shfl_sync(mask, pos, leader);
+        }
+        link = 0xFFFFFFFFu;
+        if (j < from_bump) {
+            link = base + j;
+        }
+        unsigned int fe = 0;
+        if (got_free > 0) {
+            unsigned int jj = j - from_bump;
+            fe = hrm_rt::ring_take(_dev_ctx.rings, _dev_ctx.ctl, FN, pos, (j >= from_bump) ? jj : 0xFFFFFFFFu, got_free);
+            if (j >= from_bump && jj < got_free) link = fe ? hrm_rt::entry_link(fe) : 0xFFFFFFFFu;
+        }
+        return from_bump + got_free;
+    }
+
+    // Lane-cooperative: lanes j < n return link `link` to the free ring.
+    __device__ void free_links_coop(unsigned int link, unsigned int j, unsigned int n, unsigned int mask) {
+        hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, FN, hrm_rt::encode_link(link, 1), j, n, mask);
+    }
+
+    __device__ __forceinline__ unsigned int* link_word_ptr(unsigned int link, unsigned int w, unsigned int lane) {
+        return _dev_ctx.link_words + ((size_t)link * LINK_WORDS + w) * 32u + lane;
+    }
+
+    // prog.async<F>: coalesce the active lanes' calls into F's ring.
+    template <typename TYPE>
+    __device__ __forceinline__ void push_promise(const Promise<TYPE>& p) {
+        constexpr unsigned int F = disc_of<TYPE>();
+        constexpr unsigned int W = Promise<TYPE>::WORDS;
+        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        unsigned int w[W];
+        p.to_words(w);
+        const unsigned int mask = __activemask();
+        const unsigned int rank = __popc(mask & util::lanemask_lt());
+        const unsigned int leader = __ffs(mask) - 1;
+        GroupContext& g = _grp_ctx;
+        unsigned int base = 0;
+        if (rank == 0) base = atomicAdd(&g.count[F], (unsigned int)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        const unsigned int idx = base + rank;
+        const unsigned int over = __ballot_sync(mask, idx >= RING);
+        if (idx < RING) {
+            const unsigned int slot = (g.bottom[F] + idx) & (RING - 1);
+#pragma unroll
+            for (unsigned int i = 0; i < W; i++) g.words[OFF + i][slot] = w[i];
+        }
+        if (over != 0 && idx >= RING) {
+            overflow_to_arena<TYPE>(w, over);
+        }
+    }
+
+    // Lanes in `over` could not fit in shared memory: write them straight to one arena link
+    // and publish it to the function's queue.
+    template <typename TYPE>
+    __device__ __noinline__ void overflow_to_arena(const unsigned int (&w)[Promise<TYPE>::WORDS], unsigned int over) {
+        constexpr unsigned int F = disc_of<TYPE>();
+        constexpr unsigned int W = Promise<TYPE>::WORDS;
+        const unsigned int r = __popc(over & util::lanemask_lt());
+        const unsigned int n = __popc(over);
+        unsigned int link = 0xFFFFFFFFu;
+        unsigned int got = alloc_links_coop(1, r, over, link);
+        link = __shfl_sync(over, link, __ffs(over) - 1);
+        if (got == 0 || link == 0xFFFFFFFFu) {
+            // No shared-memory slot and no arena link: the promises cannot be kept.
+            if (r == 0) hrm_rt::raise_flag(_dev_ctx.ctl, hrm_rt::ARENA_EXHAUSTED_FLAG);
+            return;
+        }
+#pragma unroll
+        for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, r), w[i]);
+        __threadfence();
+        __syncwarp(over);
+        hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, n), r, 1, over);
+    }
+
+    // -----------------------------------------------------------------------------------
+    // Arena links held outside the queues (remapping barriers).
+    // -----------------------------------------------------------------------------------
+    static const unsigned int NULL_LINK = 0xFFFFFFFFu;
+
+    // The lanes of `mask` (all calling with promises of TYPE) store their promises into one
+    // fresh arena link, in rank order. Returns the link to every lane, or NULL_LINK if the
+    // arena is exhausted (ARENA_EXHAUSTED_FLAG raised).
+    template <typename TYPE>
+    __device__ unsigned int hold_in_link(const Promise<TYPE>& p, unsigned int mask) {
+        constexpr unsigned int W = Promise<TYPE>::WORDS;
+        unsigned int w[W];
+        p.to_words(w);
+        const unsigned int r = __popc(mask & util::lanemask_lt());
+        const unsigned int leader = __ffs(mask) - 1;
+        unsigned int link = NULL_LINK;
+        unsigned int got = alloc_links_coop(1, r, mask, link);
+        link = __shfl_sync(mask, link, leader);
+        if (got == 0 || link == NULL_LINK) {
+            if (r == 0) hrm_rt::raise_flag(_dev_ctx.ctl, hrm_rt::ARENA_EXHAUSTED_FLAG);
+            return NULL_LINK;
+        }
+#pragma unroll
+        for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, r), w[i]);
+        if (r == 0) {
+            _dev_ctx.link_meta[2u * link + 0u] = 0u;
+            _dev_ctx.link_meta[2u * link + 1u] = (unsigned int)__popc(mask);
+        }
+        __threadfence();
+        __syncwarp(mask);
+        return link;
+    }
+
+    __device__ __forceinline__ unsigned int* link_next_ptr(unsigned int link) { return &_dev_ctx.link_meta[2u * link]; }
+    __device__ __forceinline__ unsigned int link_count(unsigned int link) {
+        return hrm_rt::ld_relaxed(&_dev_ctx.link_meta[2u * link + 1u]);
+    }
+
+    // One lane: publishes a held link of function f to its queue.
+    __device__ void publish_link(unsigned int f, unsigned int link, unsigned int count) {
+        const unsigned int me = 1u << util::lane_id();
+        hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, f, hrm_rt::encode_link(link, count), 0, 1, me);
+    }
+
+    template <unsigned int I>
+    __device__ __forceinline__ void push_enum(OpDisc disc, PromiseUnionType& u) {
+        if constexpr (I < FN) {
+            using Op = typename OpAt<I, OpSet>::type;
+            if (disc == I) {
+                push_promise<Op>(u.template cast<Op>());
+            } else {
+                push_enum<I + 1>(disc, u);
+            }
+        } else {
+            atomicOr(&_dev_ctx.ctl->flags, BAD_FUNC_ID_FLAG);
+        }
+    }
+
+    // ===================================================================================
+    // Scheduler (whole team converged).
+    // ===================================================================================
+
+    // Moves the oldest min(count, nlinks*32) promises of function f to the arena.
+    template <unsigned int F>
+    __device__ void spill_typed(unsigned int nlinks, unsigned long long& spilled) {
+        using Op = typename OpAt<F, OpSet>::type;
+        constexpr unsigned int W = Promise<Op>::WORDS;
+        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        GroupContext& g = _grp_ctx;
+        const unsigned int lane = util::lane_id();
+        unsigned int cnt = g.count[F];
+        unsigned int n = min(cnt, nlinks * 32u);
+        if (n == 0) return;
+        unsigned int nl = (n + 31u) / 32u;
+        unsigned int link = 0xFFFFFFFFu;
+        unsigned int got = alloc_links_coop(nl, lane, 0xFFFFFFFFu, link);
+        if (got < nl) {
+            // Return what we obtained and keep the promises in shared memory.
+            if (got > 0) free_links_coop(link, lane, got, 0xFFFFFFFFu);
+            return;
+        }
+        const unsigned int bottom = g.bottom[F];
+        for (unsigned int l = 0; l < nl; l++) {
+            unsigned int dst = __shfl_sync(0xFFFFFFFFu, link, l);
+            unsigned int k = l * 32u + lane;
+            if (k < n) {
+                unsigned int slot = (bottom + k) & (RING - 1);
+#pragma unroll
+                for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(dst, i, lane), g.words[OFF + i][slot]);
+            }
+        }
+        __threadfence();
+        __syncwarp();
+        unsigned int cnt_l = (lane < nl) ? min(32u, n - lane * 32u) : 1u;
+        hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, cnt_l), lane, nl, 0xFFFFFFFFu);
+        __syncwarp();
+        if (lane == 0) {
+            g.bottom[F] = (bottom + n) & (RING - 1);
+            g.count[F] = cnt - n;
+        }
+        __syncwarp();
+        spilled += nl;
+    }
+
+    template <unsigned int I>
+    __device__ void spill_fn(unsigned int f, unsigned int nlinks, unsigned long long& spilled) {
+        if constexpr (I < FN) {
+            if (f == I) spill_typed<I>(nlinks, spilled);
+            else spill_fn<I + 1>(f, nlinks, spilled);
+        }
+    }
+
+    // Pulls links of function F from the arena until the ring holds >= 32 promises or the
+    // queue is empty. Returns the number of links taken.
+    template <unsigned int F>
+    __device__ unsigned int fill_typed() {
+        using Op = typename OpAt<F, OpSet>::type;
+        constexpr unsigned int W = Promise<Op>::WORDS;
+        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        GroupContext& g = _grp_ctx;
+        const unsigned int lane = util::lane_id();
+        unsigned int cnt = g.count[F];
+        unsigned int room = (RING - cnt) / 32u;   // links that surely fit
+        unsigned int want = min(room, 2u);
+        if (want == 0) return 0;
+        unsigned int pos = 0, take = 0;
+        if (lane == 0) take = hrm_rt::ring_reserve(_dev_ctx.rings, F, want, pos);
+        take = __shfl_sync(0xFFFFFFFFu, take, 0);
+        if (take == 0) return 0;
+        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+        unsigned int e = hrm_rt::ring_take(_dev_ctx.rings, _dev_ctx.ctl, F, pos, lane, take);
+        __threadfence();
+        __syncwarp();
+        const unsigned int bottom = g.bottom[F];
+        for (unsigned int l = 0; l < take; l++) {
+            unsigned int el = __shfl_sync(0xFFFFFFFFu, e, l);
+            if (el == 0) continue;  // timed-out take: flag raised
+            unsigned int src = hrm_rt::entry_link(el);
+            unsigned int k = hrm_rt::entry_count(el);
+            if (lane < k) {
+                unsigned int slot = (bottom + cnt + lane) & (RING - 1);
+#pragma unroll
+                for (unsigned int i = 0; i < W; i++) g.words[OFF + i][slot] = __ldcg(link_word_ptr(src, i, lane));
+            }
+            cnt += k;
+        }
+        __syncwarp();
+        if (lane == 0) g.count[F] = cnt;
+        // Give the links back to the free ring. (After a timed-out take the link is unknown
+        // and stays out of circulation; the error flag is already raised.)
+        bool all_valid = __all_sync(0xFFFFFFFFu, lane >= take || e != 0);
+        if (all_valid) free_links_coop(lane < take ? hrm_rt::entry_link(e) : 0u, lane, take, 0xFFFFFFFFu);
+        __syncwarp();
+        return take;
+    }
+
+    template <unsigned int I>
+    __device__ unsigned int fill_fn(unsigned int f) {
+        if constexpr (I < FN) {
+            if (f == I) return fill_typed<I>();
+            return fill_fn<I + 1>(f);
+        } else {
+            return 0;
+        }
+    }
+
+    // Pops the newest k promises of function F and evaluates them, one per lane.
+    template <unsigned int F>
+    __device__ __forceinline__ void run_typed(unsigned int k) {
+        using Op = typename OpAt<F, OpSet>::type;
+        constexpr unsigned int W = Promise<Op>::WORDS;
+        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        GroupContext& g = _grp_ctx;
+        const unsigned int lane = util::lane_id();
+        const unsigned int cnt = g.count[F];
+        Promise<Op> p;
+        if (lane < k) {
+            unsigned int w[W];
+            unsigned int slot = (g.bottom[F] + cnt - k + lane) & (RING - 1);
+#pragma unroll
+            for (unsigned int i = 0; i < W; i++) w[i] = g.words[OFF + i][slot];
+            p.from_words(w);
+        }
+        __syncwarp();
+        if (lane == 0) g.count[F] = cnt - k;
+        __syncwarp();
+        if (lane < k) {
+            p(*this);
+        }
+        __syncwarp();
+    }
+
+    template <unsigned int I>
+    __device__ __forceinline__ void run_fn(unsigned int f, unsigned int k) {
+        if constexpr (I < FN) {
+            if (f == I) run_typed<I>(k);
+            else run_fn<I + 1>(f, k);
+        }
+    }
+
+    // Counts above RING mean the excess went to the arena: clamp.
+    __device__ __forceinline__ void clamp_counts() {
+        __syncwarp();
+        const unsigned int lane = util::lane_id();
+        if (lane < FN) {
+            unsigned int c = _grp_ctx.count[lane];
+            if (c > RING) _grp_ctx.count[lane] = RING;
+        }
+        __syncwarp();
+    }
+
+    // Busy/idle accounting and quiescence detection (lane 0 only).
+    // Returns 2 = quiescent (or another team declared it), 1 = work may be available, 0 = idle.
+    __device__ unsigned int idle_poll(bool& counted_idle, unsigned int& backoff) {
+        hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
+        if (!counted_idle) {
+            __threadfence();
+            atomicAdd(&ctl->busy_epoch, (unsigned long long)(-(long long)hrm_rt::BUSY_ONE));
+            counted_idle = true;
+        }
+        if (hrm_rt::ld_acquire(&ctl->done) != 0) return 2;
+        unsigned long long s1 = hrm_rt::ld_acquire64(&ctl->busy_epoch);
+        bool any = false;
+        for (unsigned int f = 0; f < FN; f++) {
+            if (hrm_rt::ld_acquire(&_dev_ctx.rings.heads[f].avail) != 0) any = true;
+        }
+        if (any) {
+            atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
+            counted_idle = false;
+            backoff = 32;
+            return 1;
+        }
+        if ((s1 >> 40) == 0) {
+            unsigned long long s2 = hrm_rt::ld_acquire64(&ctl->busy_epoch);
+            if (s2 == s1) {
+                atomicExch(&ctl->done, 1u);
+                return 2;
+            }
+        }
+        __nanosleep(backoff);
+        if (backoff < 2048) backoff <<= 1;
+        return 0;
+    }
+
+    __device__ void init_team() {
+        const unsigned int lane = util::lane_id();
+        if (lane < FN) {
+            _grp_ctx.count[lane] = 0;
+            _grp_ctx.bottom[lane] = 0;
+        }
+        __syncwarp();
+    }
+
+    // The persistent scheduling loop of one team (async.h:2625-2668 / :2155-2319).
+    __device__ void exec(unsigned int cycle_count) {
+        const unsigned int lane = util::lane_id();
+        _thd_ctx.thread_id = blockIdx.x * blockDim.x + threadIdx.x;
+        _thd_ctx.rand_state = _thd_ctx.thread_id;
+        init_team();
+        hrm_rt::call_initialize<PROGRAM_SPEC>(*this);
+        __syncwarp();
+
+        GroupContext& g = _grp_ctx;
+        hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
+        bool can_make_work = true;
+        bool counted_idle = false;
+        unsigned int backoff = 32;
+        unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_spill = 0, n_fill = 0, n_mw = 0, n_idle = 0;
+        bool quiescent = false;
+
+        for (unsigned int cycle = 0; cycle < cycle_count; cycle++) {
+            // Stop on a halt request or an error flag.
+            if ((cycle & 31u) == 0) {
+                unsigned int fl = 0;
+                if (lane == 0) fl = hrm_rt::ld_relaxed(&ctl->flags);
+                fl = __shfl_sync(0xFFFFFFFFu, fl, 0);
+                if (fl & (EARLY_HALT_FLAG | hrm_rt::ERROR_MASK)) break;
+            }
+
+            // Pick the fullest function.
+            unsigned int c = (lane < FN) ? g.count[lane] : 0u;
+            unsigned int key = (lane < FN) ? ((min(c, 0xFFFFu) << 5) | lane) : 0u;
+            unsigned int best = __reduce_max_sync(0xFFFFFFFFu, key);
+            unsigned int bf = best & 31u, bc = best >> 5;
+
+            if (bc < 32u) {
+                // No full batch locally: try the arena for the function closest to full.
+                unsigned int av = 0;
+                if (lane < FN) av = hrm_rt::ld_relaxed(&_dev_ctx.rings.heads[lane].avail);
+                unsigned int fkey = (lane < FN && (int)av > 0) ? (((min(c, 0xFFFFu) + 1u) << 5) | lane) : 0u;
+                unsigned int fbest = __reduce_max_sync(0xFFFFFFFFu, fkey);
+                if (fbest != 0) {
+                    unsigned int ff = fbest & 31u;
+                    if (counted_idle) {
+                        if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
+                        counted_idle = false;
+                    }
+                    unsigned int took = fill_fn<0>(ff);
+                    n_fill += took;
+                    if (took > 0) continue;
+                }
+                if (can_make_work) {
+                    if (counted_idle) {
+                        if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
+                        counted_idle = false;
+                    }
+                    bool more = hrm_rt::call_make_work<PROGRAM_SPEC>(*this);
+                    can_make_work = __any_sync(0xFFFFFFFFu, more);
+                    n_mw++;
+                    clamp_counts();
+                    continue;
+                }
+                if (bc == 0) {
+                    // Nothing local, nothing in the arena, nothing to make: idle.
+                    unsigned int st = 0;
+                    if (lane == 0) st = idle_poll(counted_idle, backoff);
+                    st = __shfl_sync(0xFFFFFFFFu, st, 0);
+                    counted_idle = __shfl_sync(0xFFFFFFFFu, (unsigned int)counted_idle, 0) != 0;
+                    n_idle++;
+                    if (st == 2) { quiescent = true; break; }
+                    continue;
+                }
+            }
+
+            // Evaluate one batch (full when possible).
+            if (counted_idle) {
+                if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
+                counted_idle = false;
+            }
+            unsigned int k = min(bc, 32u);
+            // Every other ring needs one link of headroom for the calls this batch makes
+            // (the batch's own ring frees k slots when it is popped).
+            unsigned int hi = __ballot_sync(0xFFFFFFFFu, lane < FN && lane != bf && c > RING - 32u);
+            while (hi) {
+                unsigned int f = __ffs(hi) - 1;
+                hi &= hi - 1;
+                unsigned int cf = __shfl_sync(0xFFFFFFFFu, c, f);
+                spill_fn<0>(f, (cf - (RING - 32u) + 31u) / 32u, n_spill);
+            }
+            run_fn<0>(bf, k);
+            clamp_counts();
+            n_evals += k;
+            n_batches += 1;
+            n_full += (k == 32u);
+        }
+
+        hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
+        __syncwarp();
+
+        // Leave nothing in shared memory: spill every pending promise.
+        for (unsigned int f = 0; f < FN; f++) {
+            unsigned int cf = g.count[f];
+            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
+        }
+        if (lane == 0) {
+            if (can_make_work) atomicOr(&ctl->flags, EARLY_HALT_FLAG);
+            for (unsigned int f = 0; f < FN; f++) {
+                if (g.count[f] != 0) atomicOr(&ctl->flags, hrm_rt::ARENA_EXHAUSTED_FLAG);
+            }
+            if (!counted_idle) {
+                __threadfence();
+                atomicAdd(&ctl->busy_epoch, (unsigned long long)(-(long long)hrm_rt::BUSY_ONE));
+            }
+            unsigned long long* st = _dev_ctx.stats;
+            atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);
+            atomicAdd(&st[hrm_rt::STAT_BATCHES], n_batches);
+            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], n_full);
+            atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], n_spill);
+            atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], n_fill);
+            atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], n_mw);
+            atomicAdd(&st[hrm_rt::STAT_IDLE_POLLS], n_idle);
+            (void)quiescent;
+            __threadfence();
+            unsigned int out = atomicAdd(&ctl->checkout, 1u);
+            if (out == ctl->total_teams - 1u) {
+                // Last team out decides completion.
+                __threadfence();
+                unsigned int old = atomicAnd(&ctl->flags, ~EARLY_HALT_FLAG);
+                unsigned int done = hrm_rt::ld_acquire(&ctl->done);
+                bool left = false;
+                for (unsigned int f = 0; f < FN; f++) {
+                    if (hrm_rt::ld_acquire(&_dev_ctx.rings.heads[f].avail) != 0) left = true;
+                }
+                if (done && !left && !(old & (EARLY_HALT_FLAG | hrm_rt::ERROR_MASK))) {
+                    atomicOr(&ctl->flags, COMPLETION_FLAG);
+                }
+            }
+        }
+    }
+
+    // Device side of init<P>: reset queues, arena and control block (async.h:2405-2516).
+    __device__ static void init_program(DeviceContext ctx) {
+        size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        size_t nthreads = (size_t)gridDim.x * blockDim.x;
+        hrm_rt::ring_init_slots(ctx.rings, FN + 1, tid, nthreads);
+        if (tid == 0) {
+            ctx.ctl->flags = 0;
+            ctx.ctl->checkout = 0;
+            ctx.ctl->done = 0;
+            ctx.ctl->bump = 0;
+            ctx.ctl->arena_links = ctx.arena_links;
+            ctx.ctl->busy_epoch = 0;
+        }
+        if (tid < hrm_rt::STAT_COUNT) ctx.stats[tid] = 0;
+    }
+
+    // ===================================================================================
+    // Host launch helpers used by init<P> and exec<P>.
+    // ===================================================================================
+    static unsigned int resident_ctas() {
+        static int cached_dev = -1;
+        static unsigned int cached = 0;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev != cached_dev) {
+            cached = hrm_rt::max_resident_ctas(hrm_rt::async_exec_kernel<ProgramType>, (int)CTA_THREADS, 0);
+            cached_dev = dev;
+        }
+        return cached;
+    }
+
+    // Number of CTAs exec<P> launches for `group_count` work groups.
+    static unsigned int ctas_for(size_t group_count) {
+        size_t want = (group_count + TEAMS_PER_CTA - 1) / TEAMS_PER_CTA;
+        if (want == 0) want = 1;
+        unsigned int cap = resident_ctas();
+        if (cap == 0) cap = 1;
+        return (unsigned int)(want < cap ? want : cap);
+    }
+
+    static void launch_init(Instance& inst, size_t, cudaStream_t stream) {
+        hrm_rt::async_init_kernel<ProgramType><<<148, 256, 0, stream>>>(inst.to_context());
+    }
+
+    static void launch_exec(Instance& inst, size_t group_count, size_t cycle_count, cudaStream_t stream) {
+        unsigned int ctas = ctas_for(group_count);
+        unsigned int cycles = cycle_count > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned int)cycle_count;
+        DeviceContext ctx = inst.to_context();
+        hrm_rt::async_prep_kernel<ProgramType><<<1, 32, 0, stream>>>(ctx, ctas * TEAMS_PER_CTA);
+        hrm_rt::async_exec_kernel<ProgramType><<<ctas, CTA_THREADS, 0, stream>>>(ctx, inst.device_state, cycles);
+    }
+};
+
+namespace hrm_rt {
+
+template <typename PROG>
+__global__ void async_init_kernel(typename PROG::DeviceContext ctx) {
+    PROG::init_program(ctx);
+}
+
+// Resets the per-exec counters before the persistent kernel starts.
+template <typename PROG>
+__global__ void async_prep_kernel(typename PROG::DeviceContext ctx, unsigned int total_teams) {
+    if (threadIdx.x == 0) {
+        ctx.ctl->checkout = 0;
+        ctx.ctl->done = 0;
+        ctx.ctl->total_teams = total_teams;
+        ctx.ctl->busy_epoch = (unsigned long long)total_teams << 40;
+        atomicAnd(&ctx.ctl->flags, ~COMPLETION_FLAG);
+        __threadfence();
+    }
+}
+
+template <typename PROG>
+__global__ void __launch_bounds__(PROG::CTA_THREADS, PROG::MIN_CTAS_PER_SM)
+    async_exec_kernel(typename PROG::DeviceContext ctx, typename PROG::DeviceState device, unsigned int cycles) {
+    __shared__ typename PROG::GroupContext grp_ctx[PROG::TEAMS_PER_CTA];
+    __shared__ typename PROG::GroupState grp_state[PROG::TEAMS_PER_CTA];
+    const unsigned int team = threadIdx.x >> 5;
+    typename PROG::ThreadContext thd_ctx;
+    typename PROG::ThreadState thd_state;
+    PROG prog(ctx, grp_ctx[team], thd_ctx, device, grp_state[team], thd_state);
+    prog.exec(cycles);
+}
+
+}  // namespace hrm_rt
+
+#endif
