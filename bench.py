@@ -1,0 +1,432 @@
+"""Benchmark of the B200-native Harmonize runtime (one JSON line on stdout, rank 0).
+
+Default workload: the Monte Carlo photon walk — 10^7 photons of weight 1 launched at the
+centre of a 128^3 grid of unit voxels (seeded synthetic medium), AsyncProgram. One step is
+one complete run of that batch through the runtime's C ABI. Metric: async calls/s (one
+call = one eval), whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload photon|bfs|collatz] [--program async|event]
+
+value : calls / device time with inputs resident in HBM (hrm_*_run_device), CUDA events on
+        the launching (default) stream, L2 flushed before every step (untimed).
+e2e   : the same metric through the host-buffer entry point (hrm_*_run): input upload and
+        result download inside the timed region, pinned host memory.
+--gpus N under torchrun: one independent replica per GPU (the walk has no cross-replica
+exchange), photon ids offset per rank (weak scaling); time = max over ranks.
+--impl reference: the reference runtime (Harmonize's own AsyncProgram, built from its
+headers with the same spec source into oracle/_ref) on the same workload and metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="photon", choices=["photon", "bfs", "collatz"])
+    p.add_argument("--program", default="async", choices=["async", "event"])
+    p.add_argument("--photons", type=int, default=10_000_000)
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--variant", type=int, default=-1, help="compiled tuning variant (-1 = autotuned)")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": PEAKS_FALLBACK["hbm_gbs"], "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    import torch
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, value):
+    import torch
+    if pg is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, value):
+    import torch
+    if pg is None:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def flush_l2(buf):
+    buf.zero_()  # 256 MiB > the 126 MB L2
+
+
+# ---------------------------------------------------------------------------------------
+# Algorithmic bytes per call (roofline accounting). A queued promise is written once and
+# read once; each function then touches its compulsory application bytes.
+#   photon Move    : 2 x 44 B promise + 4 B mu_s + 1 B split flag          =  93 B
+#   photon Collide : 2 x 44 B promise + 4 B absorb                          =  92 B
+#   photon Tally   : 2 x 16 B promise + 16 B uint64 read-modify-write       =  48 B
+#   BFS Relax      : 2 x 8 B promise + 8 B level read-modify-write          =  24 B
+#   BFS Expand     : 2 x 12 B promise + 8 B rowptr + 4 B per edge read (counted on Relax side: 4 B)
+#   Collatz Even/Odd: 2 x 16 B promise (+ 4 B output once per start, ignored) = 32 B
+# ---------------------------------------------------------------------------------------
+BYTES_PER_CALL = {
+    "photon": [93, 92, 48],
+    "bfs": [24 + 4, 24 + 8],
+    "collatz": [32, 32],
+}
+
+
+def run_photon(args, hrm, rank, world, pg, torch):
+    n = args.grid
+    count = args.photons
+    first = rank * count
+    seed = 0x5EED0123456789
+    mu, ab, sp = hrm.photon_medium(n, 2024)
+    nvox = n ** 3
+    slots = nvox + 3 * hrm.PHOTON_SPREAD
+    d_mu = torch.from_numpy(mu).cuda()
+    d_ab = torch.from_numpy(ab).cuda()
+    d_sp = torch.from_numpy(sp).cuda()
+    d_tally = torch.zeros(slots, dtype=torch.int64, device="cuda")
+    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    L = hrm.lib()
+
+    def step_device():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_photon_run_device(d_mu.data_ptr(), d_ab.data_ptr(), d_sp.data_ptr(), n, seed, first, count,
+                                          d_tally.data_ptr(), ctypes.byref(cfg), ctypes.byref(res)))
+        return res.as_dict()
+
+    h_mu = torch.from_numpy(mu).pin_memory()
+    h_ab = torch.from_numpy(ab).pin_memory()
+    h_sp = torch.from_numpy(sp).pin_memory()
+    h_tally = torch.zeros(slots, dtype=torch.int64).pin_memory()
+
+    def step_e2e():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_photon_run(h_mu.data_ptr(), h_ab.data_ptr(), h_sp.data_ptr(), n, seed, first, count,
+                                   h_tally.data_ptr(), ctypes.byref(cfg), ctypes.byref(res)))
+        return res.as_dict()
+
+    def checksum():
+        t = d_tally.cpu().numpy().view(np.uint64)
+        total = (int(t[:nvox].sum()) + int(t[nvox:nvox + 1024].sum()) + int(t[nvox + 1024:nvox + 2048].sum())
+                 - int(t[nvox + 2048:].sum()))
+        return int(t.sum(dtype=np.uint64)), total / 2.0 ** 32
+
+    def cpu_sample(target_s=10.0):
+        import oracle
+        threads = oracle.max_threads()
+        k = 2000
+        t0 = time.perf_counter()
+        _, calls = oracle.exec_photon(mu, ab, sp, n, seed, first, k, threads=threads)
+        dt = time.perf_counter() - t0
+        k2 = int(min(2_000_000, max(k, k * target_s / max(dt, 1e-3))))
+        t0 = time.perf_counter()
+        _, calls = oracle.exec_photon(mu, ab, sp, n, seed, first, k2, threads=threads)
+        dt = time.perf_counter() - t0
+        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+                "sample": f"{k2} photons of the same 128^3 medium, OpenMP host executor of the same spec source, "
+                          f"{int(calls.sum())} calls in {dt:.2f} s"}
+
+    config = {"workload": f"photon_walk_{count:.0e}_photons_{n}^3", "photons_per_gpu": count, "grid": n,
+              "program": args.program, "l2": "flushed before every step (256 MiB write)",
+              "medium": "seeded synthetic: mu_s~lognormal(0,0.5), absorb~U[0.02,0.2], split p=0.1"}
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
+                config=config, h2d=int(mu.nbytes + ab.nbytes + sp.nbytes), d2h=int(slots * 8), dtype="f32",
+                bytes_per_call=BYTES_PER_CALL["photon"], launches_per_step=3 if args.program == "async" else 2)
+
+
+def run_bfs(args, hrm, rank, world, pg, torch):
+    rp, col = hrm.rmat_csr(args.scale, 16, 0.57, 0.19, 0.19, 1)
+    nv = len(rp) - 1
+    d_rp = torch.from_numpy(rp.view(np.int32)).cuda()
+    d_col = torch.from_numpy(col.view(np.int32)).cuda()
+    d_lev = torch.empty(nv, dtype=torch.int32, device="cuda")
+    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    L = hrm.lib()
+
+    def step_device():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_bfs_run_device(d_rp.data_ptr(), d_col.data_ptr(), nv, 0, d_lev.data_ptr(), ctypes.byref(cfg),
+                                       ctypes.byref(res)))
+        return res.as_dict()
+
+    h_rp = torch.from_numpy(rp.view(np.int32)).pin_memory()
+    h_col = torch.from_numpy(col.view(np.int32)).pin_memory()
+    h_lev = torch.empty(nv, dtype=torch.int32).pin_memory()
+
+    def step_e2e():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_bfs_run(h_rp.data_ptr(), h_col.data_ptr(), nv, 0, h_lev.data_ptr(), ctypes.byref(cfg),
+                                ctypes.byref(res)))
+        return res.as_dict()
+
+    def checksum():
+        lv = d_lev.cpu().numpy().view(np.uint32)
+        return int(lv.astype(np.uint64).sum()), int((lv != 0xFFFFFFFF).sum())
+
+    def cpu_sample(target_s=10.0):
+        import oracle
+        threads = oracle.max_threads()
+        t0 = time.perf_counter()
+        _, calls = oracle.exec_bfs(rp, col, 0, threads=threads)
+        dt = time.perf_counter() - t0
+        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+                "sample": f"full R-MAT 2^{args.scale} BFS, OpenMP host executor of the same spec source"}
+
+    config = {"workload": f"rmat_bfs_2^{args.scale}_ef16", "vertices": nv, "edges": int(len(col)),
+              "program": args.program, "l2": "flushed before every step (256 MiB write)"}
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
+                config=config, h2d=int(rp.nbytes + col.nbytes), d2h=int(nv * 4), dtype="u32",
+                bytes_per_call=BYTES_PER_CALL["bfs"], launches_per_step=3 if args.program == "async" else 2)
+
+
+def run_collatz(args, hrm, rank, world, pg, torch):
+    count = 1 << 20
+    start = 1 + rank * count
+    d_out = torch.empty(count, dtype=torch.int32, device="cuda")
+    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    L = hrm.lib()
+
+    def step_device():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_collatz_run_device(start, count, d_out.data_ptr(), ctypes.byref(cfg), ctypes.byref(res)))
+        return res.as_dict()
+
+    h_out = torch.empty(count, dtype=torch.int32).pin_memory()
+
+    def step_e2e():
+        res = hrm.RunResult()
+        hrm.check(L.hrm_collatz_run(start, count, h_out.data_ptr(), ctypes.byref(cfg), ctypes.byref(res)))
+        return res.as_dict()
+
+    def checksum():
+        o = d_out.cpu().numpy().view(np.uint32)
+        return int(o.astype(np.uint64).sum()), int(o.max())
+
+    def cpu_sample(target_s=10.0):
+        import oracle
+        threads = oracle.max_threads()
+        t0 = time.perf_counter()
+        _, calls = oracle.exec_collatz(start, count, threads=threads)
+        dt = time.perf_counter() - t0
+        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+                "sample": "n = 1..2^20, OpenMP host executor of the same spec source"}
+
+    config = {"workload": "collatz_1_to_2^20", "starts": count, "program": args.program,
+              "l2": "flushed before every step (256 MiB write)"}
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
+                config=config, h2d=0, d2h=count * 4, dtype="u64",
+                bytes_per_call=BYTES_PER_CALL["collatz"], launches_per_step=3 if args.program == "async" else 2)
+
+
+def pick_variant(args, hrm):
+    """--variant, else the autotuner's choice for this workload and program type."""
+    if args.variant >= 0:
+        return args.variant
+    from harmonize_b200.autotune import tuned_variant
+    return tuned_variant(args.workload, args.program)
+
+
+def algorithmic_bytes(stats, per_call):
+    return sum(stats.get(f"fn{i}_evals", 0) * b for i, b in enumerate(per_call))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        from oracle import reference_bench
+        return reference_bench.main(args)
+    import torch
+    import harmonize_b200 as hrm
+    rank, world, local, pg = dist_setup(args)
+    wl = {"photon": run_photon, "bfs": run_bfs, "collatz": run_collatz}[args.workload](args, hrm, rank, world, pg,
+                                                                                       torch)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(max(args.warmup, 0)):
+        wl["step_device"]()
+    ref_sum = wl["checksum"]()
+
+    # Timed device-resident steps.
+    barrier(pg)
+    step_ms, stats_all = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st = wl["step_device"]()
+            e1.record()
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            stats_all.append(st)
+            if wl["checksum"]() != ref_sum:
+                raise SystemExit("bench: results differ between steps (determinism violated)")
+    barrier(pg)
+    my_ms = sum(step_ms)
+    total_ms = max_over_ranks(pg, my_ms)
+    calls = sum(s["evals"] for s in stats_all)
+    all_calls = sum_over_ranks(pg, calls)
+    value = all_calls / (total_ms / 1e3)
+
+    # End-to-end through the host-buffer entry point.
+    wl["step_e2e"]()
+    barrier(pg)
+    e2e_ms = []
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = wl["step_e2e"]()
+        e1.record()
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    barrier(pg)
+    e2e_total = max_over_ranks(pg, sum(e2e_ms))
+    e2e_calls = sum_over_ranks(pg, st["evals"] * e2e_steps)
+    e2e_value = e2e_calls / (e2e_total / 1e3)
+
+    pk = peaks()
+    s0 = stats_all[-1]
+    alg = algorithmic_bytes(s0, wl["bytes_per_call"])
+    achieved_gbs = alg / (step_ms[-1] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": None,
+                "peak_source": pk["source"],
+                "algorithmic_bytes_per_launch": alg,
+                "note": "algorithmic bytes = each call's promise written and read once plus its compulsory "
+                        "application bytes; the launch duration is the whole run (init + exec kernels)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = wl["cpu_sample"]()
+        except Exception as e:  # the CPU leg is a reported baseline only
+            cpu = {"value": None, "error": str(e)}
+    if rank == 0:
+        full = s0.get("full_batches", 0) / max(1, s0.get("batches", 1))
+        line = {
+            "metric": "async calls/s", "value": round(value, 1), "unit": "calls/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
+            "data": "synthetic",
+            "config": dict(wl["config"], parallelism=f"replicas x{world}",
+                           variant={"id": pick_variant(args, hrm), "ring_links_teams_per_cta":
+                                    list(hrm.VARIANTS[pick_variant(args, hrm)])}),
+            "e2e": {"value": round(e2e_value, 1), "unit": "calls/s", "h2d_bytes_per_step": wl["h2d"],
+                    "d2h_bytes_per_step": wl["d2h"]},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": wl["launches_per_step"] * args.steps,
+            "runtime_stats": {"calls_per_step": s0["evals"], "full_batch_fraction": round(full, 4),
+                              "spill_links": s0.get("spill_links"), "fill_links": s0.get("fill_links"),
+                              "execs": s0.get("execs")},
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -31,7 +31,7 @@ FLAG_EARLY_HALT = 0x40000000
 FLAG_COMPLETION = 0x80000000
 
 STAT_NAMES = ["evals", "batches", "full_batches", "spill_links", "fill_links", "make_work",
-              "idle_polls", "generations"]
+              "idle_polls", "generations"] + [f"fn{i}_evals" for i in range(16)]
 
 
 class HarmonizeError(RuntimeError):
@@ -43,7 +43,11 @@ class HarmonizeError(RuntimeError):
 class RunConfig(ctypes.Structure):
     _fields_ = [("program_type", ctypes.c_int), ("groups", ctypes.c_size_t), ("cycles", ctypes.c_size_t),
                 ("chunk", ctypes.c_size_t), ("arena", ctypes.c_size_t), ("max_execs", ctypes.c_size_t),
-                ("stream", ctypes.c_void_p)]
+                ("stream", ctypes.c_void_p), ("variant", ctypes.c_int)]
+
+
+# Compiled tuning variants: (shared-memory ring links per function, teams per CTA).
+VARIANTS = {0: (2, 4), 1: (4, 4), 2: (4, 2), 3: (8, 2), 4: (2, 8)}
 
 
 class RunResult(ctypes.Structure):
@@ -82,6 +86,14 @@ def lib():
             "hrm_program_overview": [vp, vp, sz, ctypes.POINTER(sz)],
             "hrm_collatz_run": [u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
             "hrm_collatz_run_device": [u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
+            "hrm_photon_run": [vp, vp, vp, u32, ctypes.c_uint64, u32, u32, vp, ctypes.POINTER(RunConfig),
+                               ctypes.POINTER(RunResult)],
+            "hrm_photon_run_device": [vp, vp, vp, u32, ctypes.c_uint64, u32, u32, vp, ctypes.POINTER(RunConfig),
+                                      ctypes.POINTER(RunResult)],
+            "hrm_bfs_run": [vp, vp, u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
+            "hrm_bfs_run_device": [vp, vp, u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
+            "hrm_rmat_csr": [u32, u32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, vp, vp],
+            "hrm_photon_medium": [u32, ctypes.c_uint64, vp, vp, vp],
         }
         for name, args in sigs.items():
             f = getattr(L, name)
@@ -109,9 +121,9 @@ def exported_symbols():
     return names
 
 
-def make_config(program="async", groups=0, cycles=0, chunk=0, arena=0, max_execs=0, stream=None):
+def make_config(program="async", groups=0, cycles=0, chunk=0, arena=0, max_execs=0, stream=None, variant=0):
     pt = {"async": ASYNC, "event": EVENT}[program] if isinstance(program, str) else int(program)
-    return RunConfig(pt, groups, cycles, chunk, arena, max_execs, stream)
+    return RunConfig(pt, groups, cycles, chunk, arena, max_execs, stream, variant)
 
 
 def collatz(start, count, program="async", **kw):
@@ -123,6 +135,58 @@ def collatz(start, count, program="async", **kw):
     res = RunResult()
     check(lib().hrm_collatz_run(start, count, out.ctypes.data, ctypes.byref(cfg), ctypes.byref(res)))
     return out, res.as_dict()
+
+
+PHOTON_SPREAD = 1024
+
+
+def photon_medium(n, seed):
+    """Seeded medium of an n^3 grid: (mu_s float32, absorb float32, split uint8)."""
+    nv = n ** 3
+    mu = np.empty(nv, dtype=np.float32)
+    ab = np.empty(nv, dtype=np.float32)
+    sp = np.empty(nv, dtype=np.uint8)
+    if lib().hrm_photon_medium(n, seed, mu.ctypes.data, ab.ctypes.data, sp.ctypes.data) != 0:
+        raise HarmonizeError(HRM_EINVAL, "bad medium arguments")
+    return mu, ab, sp
+
+
+def rmat_csr(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1):
+    """Seeded R-MAT graph as CSR (rowptr uint32[2^scale+1], col uint32[E])."""
+    nv = 1 << scale
+    rowptr = np.empty(nv + 1, dtype=np.uint32)
+    col = np.empty(edge_factor * nv, dtype=np.uint32)
+    if lib().hrm_rmat_csr(scale, edge_factor, a, b, c, seed, rowptr.ctypes.data, col.ctypes.data) != 0:
+        raise HarmonizeError(HRM_EINVAL, "bad R-MAT arguments")
+    return rowptr, col
+
+
+def photon_walk(mu_s, absorb, split, n, seed, first, count, program="async", **kw):
+    """Photon walk of photons [first, first+count) from host arrays.
+
+    Returns (tally uint64[n^3 + 3*1024], run-result dict)."""
+    mu_s = np.ascontiguousarray(mu_s, dtype=np.float32)
+    absorb = np.ascontiguousarray(absorb, dtype=np.float32)
+    split = np.ascontiguousarray(split, dtype=np.uint8)
+    tally = np.zeros(n ** 3 + 3 * PHOTON_SPREAD, dtype=np.uint64)
+    cfg = make_config(program, **kw)
+    res = RunResult()
+    check(lib().hrm_photon_run(mu_s.ctypes.data, absorb.ctypes.data, split.ctypes.data, n, seed, first, count,
+                               tally.ctypes.data, ctypes.byref(cfg), ctypes.byref(res)))
+    return tally, res.as_dict()
+
+
+def bfs(rowptr, col, root=0, program="async", **kw):
+    """Breadth-first levels from `root` (uint32, unreached 0xFFFFFFFF) from host arrays."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    nv = len(rowptr) - 1
+    levels = np.empty(nv, dtype=np.uint32)
+    cfg = make_config(program, **kw)
+    res = RunResult()
+    check(lib().hrm_bfs_run(rowptr.ctypes.data, col.ctypes.data, nv, root, levels.ctypes.data, ctypes.byref(cfg),
+                            ctypes.byref(res)))
+    return levels, res.as_dict()
 
 
 class Program:

@@ -5,7 +5,9 @@
 // harmonize/python/templates.py:3-184).
 #include "../../include/harmonize.h"
 #include "../../include/hrm_capi.h"
+#include "specs/bfs.h"
 #include "specs/collatz.h"
+#include "specs/photon.h"
 
 #include <mutex>
 #include <string>
@@ -62,10 +64,9 @@ struct ProgramImpl : ProgramBase {
     std::vector<unsigned int> overview() override { return inst.overview(); }
 };
 
-using CollatzAsync = AsyncProgram<hrm_specs::CollatzSpec<>>;
-using CollatzEvent = EventProgram<hrm_specs::CollatzSpec<>>;
-
 static_assert(sizeof(hrm_collatz_state) == sizeof(hrm_specs::CollatzState), "collatz state layout");
+static_assert(sizeof(hrm_photon_state) == sizeof(hrm_specs::PhotonState), "photon state layout");
+static_assert(sizeof(hrm_bfs_state) == sizeof(hrm_specs::BfsState), "bfs state layout");
 
 template <typename STATE>
 STATE state_from(const void* p, size_t n) {
@@ -75,14 +76,49 @@ STATE state_from(const void* p, size_t n) {
     return s;
 }
 
-ProgramBase* make_program(int spec, int type, size_t arena, const void* state, size_t state_size) {
+// Instantiates spec SPEC<RING, TEAMS> for the chosen program type and tuning variant.
+template <template <size_t, size_t> class SPEC, typename STATE>
+ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
+    if (type == HRM_ASYNC) {
+        switch (variant) {
+            case HRM_VARIANT_R2_T4: return new ProgramImpl<AsyncProgram<SPEC<2, 4>>>(arena, s);
+            case HRM_VARIANT_R4_T4: return new ProgramImpl<AsyncProgram<SPEC<4, 4>>>(arena, s);
+            case HRM_VARIANT_R4_T2: return new ProgramImpl<AsyncProgram<SPEC<4, 2>>>(arena, s);
+            case HRM_VARIANT_R8_T2: return new ProgramImpl<AsyncProgram<SPEC<8, 2>>>(arena, s);
+            case HRM_VARIANT_R2_T8: return new ProgramImpl<AsyncProgram<SPEC<2, 8>>>(arena, s);
+            default: break;
+        }
+    } else if (type == HRM_EVENT) {
+        switch (variant) {
+            case HRM_VARIANT_R2_T4:
+            case HRM_VARIANT_R4_T4: return new ProgramImpl<EventProgram<SPEC<2, 4>>>(arena, s);
+            case HRM_VARIANT_R4_T2:
+            case HRM_VARIANT_R8_T2: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
+            case HRM_VARIANT_R2_T8: return new ProgramImpl<EventProgram<SPEC<2, 8>>>(arena, s);
+            default: break;
+        }
+    }
+    return nullptr;
+}
+
+ProgramBase* make_program(int spec, int type, size_t arena, const void* state, size_t state_size, int variant = 0) {
     ProgramBase* p = nullptr;
     switch (spec) {
         case HRM_SPEC_COLLATZ: {
             auto s = state_from<hrm_specs::CollatzState>(state, state_size);
             if (s.leap == 0) s.leap = 1;
-            if (type == HRM_ASYNC) p = new ProgramImpl<CollatzAsync>(arena, s);
-            else if (type == HRM_EVENT) p = new ProgramImpl<CollatzEvent>(arena, s);
+            p = make_variant<hrm_specs::CollatzSpec>(type, variant, arena, s);
+            break;
+        }
+        case HRM_SPEC_PHOTON: {
+            auto s = state_from<hrm_specs::PhotonState>(state, state_size);
+            if (s.leap == 0) s.leap = 1;
+            p = make_variant<hrm_specs::PhotonSpec>(type, variant, arena, s);
+            break;
+        }
+        case HRM_SPEC_BFS: {
+            auto s = state_from<hrm_specs::BfsState>(state, state_size);
+            p = make_variant<hrm_specs::BfsSpec>(type, variant, arena, s);
             break;
         }
         default:
@@ -95,8 +131,8 @@ ProgramBase* make_program(int spec, int type, size_t arena, const void* state, s
 }
 
 size_t default_arena(int spec, int type) {
-    if (type == HRM_EVENT) return spec == HRM_SPEC_COLLATZ ? (1u << 20) : (1u << 22);
-    return 1u << 18;
+    if (type == HRM_EVENT) return spec == HRM_SPEC_COLLATZ ? (1u << 20) : (1u << 24);
+    return spec == HRM_SPEC_COLLATZ ? (1u << 18) : (1u << 20);
 }
 
 // Runs an instance to completion: init, then exec until complete or the budget ends.
@@ -180,7 +216,59 @@ int collatz_run(uint32_t start, uint32_t count, uint32_t* d_out, const hrm_run_c
     st.iterator = it.ptr;
     st.leap = 1;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_COLLATZ, cfg.program_type);
-    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_COLLATZ, cfg.program_type, arena, &st, sizeof(st)));
+    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_COLLATZ, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
+    return run_to_completion(p.get(), cfg, res);
+}
+
+// Photon walk with device-resident medium and tally (tally zeroed here).
+int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32_t n, uint64_t seed, uint32_t first,
+               uint32_t count, uint64_t* d_tally, const hrm_run_config* cfg_in, hrm_run_result* res) {
+    hrm_run_config cfg = config_or_default(cfg_in);
+    if (n < 2 || n > 1024 || (n & 1u)) return fail(HRM_EINVAL, "grid edge must be even and in [2, 1024]");
+    if ((uint64_t)first + count > 0xFFFFFFFFull) return fail(HRM_EINVAL, "first + count exceeds 2^32");
+    cudaStream_t s = (cudaStream_t)cfg.stream;
+    const size_t slots = (size_t)n * n * n + 3u * hrm_specs::PHOTON_SPREAD;
+    ck(cudaMemsetAsync(d_tally, 0, slots * sizeof(uint64_t), s), "tally clear");
+    DeviceArray<util::iter::AtomicIter<unsigned int>> it(1);
+    util::iter::AtomicIter<unsigned int> host_it(first, first + count);
+    ck(cudaMemcpyAsync(it.ptr, &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    hrm_specs::PhotonState st;
+    st.mu_s = d_mu;
+    st.absorb = d_ab;
+    st.split = d_sp;
+    st.tally = (unsigned long long*)d_tally;
+    st.source = it.ptr;
+    st.n = n;
+    st.seed_lo = (uint32_t)seed;
+    st.seed_hi = (uint32_t)(seed >> 32);
+    st.leap = 1;
+    // EventProgram launches new photons only while the move buffer is under 1/64 full:
+    // splits grow a batch of photons several-fold before roulette thins it.
+    st.load_limit = 0.015625f;
+    size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_PHOTON, cfg.program_type);
+    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_PHOTON, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
+    return run_to_completion(p.get(), cfg, res);
+}
+
+// BFS over a device-resident CSR graph; levels initialised here.
+int bfs_run(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root, uint32_t* d_levels,
+            const hrm_run_config* cfg_in, hrm_run_result* res) {
+    hrm_run_config cfg = config_or_default(cfg_in);
+    if (root >= nv) return fail(HRM_EINVAL, "root out of range");
+    cudaStream_t s = (cudaStream_t)cfg.stream;
+    ck(cudaMemsetAsync(d_levels, 0xFF, (size_t)nv * 4u, s), "levels init");
+    DeviceArray<util::iter::AtomicIter<unsigned int>> it(1);
+    util::iter::AtomicIter<unsigned int> host_it(0, 1);
+    ck(cudaMemcpyAsync(it.ptr, &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    hrm_specs::BfsState st;
+    st.rowptr = d_rowptr;
+    st.col = d_col;
+    st.levels = d_levels;
+    st.roots = it.ptr;
+    st.root = root;
+    st.nv = nv;
+    size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_BFS, cfg.program_type);
+    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_BFS, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
     return run_to_completion(p.get(), cfg, res);
 }
 
@@ -190,9 +278,9 @@ struct hrm_program {
     ProgramBase* impl;
 };
 
-#define HRM_GUARD(body)                                          \
+#define HRM_GUARD(...)                                           \
     try {                                                        \
-        body                                                     \
+        __VA_ARGS__                                              \
     } catch (std::invalid_argument & e) {                        \
         return fail(HRM_EINVAL, e.what());                       \
     } catch (DeviceFlagError & e) {                              \
@@ -221,6 +309,17 @@ int hrm_program_create(int spec, int program_type, size_t arena_or_io, const voi
     HRM_GUARD({
         size_t arena = arena_or_io ? arena_or_io : default_arena(spec, program_type);
         ProgramBase* p = make_program(spec, program_type, arena, device_state, state_size);
+        *out = new hrm_program{p};
+        return HRM_OK;
+    })
+}
+
+int hrm_program_create_variant(int spec, int program_type, int variant, size_t arena_or_io, const void* device_state,
+                               size_t state_size, hrm_program** out) {
+    if (out == nullptr) return fail(HRM_EINVAL, "out is NULL");
+    HRM_GUARD({
+        size_t arena = arena_or_io ? arena_or_io : default_arena(spec, program_type);
+        ProgramBase* p = make_program(spec, program_type, arena, device_state, state_size, variant);
         *out = new hrm_program{p};
         return HRM_OK;
     })
@@ -314,6 +413,62 @@ int hrm_collatz_run(uint32_t start, uint32_t count, uint32_t* out, const hrm_run
         if (rc != HRM_OK) return rc;
         ck(cudaMemcpyAsync(out, d.ptr, (size_t)count * 4u, cudaMemcpyDeviceToHost, s), "output download");
         ck(cudaStreamSynchronize(s), "output download");
+        return HRM_OK;
+    })
+}
+
+int hrm_photon_run_device(const float* d_mu_s, const float* d_absorb, const uint8_t* d_split, uint32_t n,
+                          uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally,
+                          const hrm_run_config* cfg, hrm_run_result* res) {
+    if (!d_mu_s || !d_absorb || !d_split || !d_tally) return fail(HRM_EINVAL, "NULL buffer");
+    HRM_GUARD(return photon_run(d_mu_s, d_absorb, d_split, n, seed, first, count, d_tally, cfg, res);)
+}
+
+int hrm_photon_run(const float* mu_s, const float* absorb, const uint8_t* split, uint32_t n, uint64_t seed,
+                   uint32_t first, uint32_t count, uint64_t* tally, const hrm_run_config* cfg_in,
+                   hrm_run_result* res) {
+    if (!mu_s || !absorb || !split || !tally) return fail(HRM_EINVAL, "NULL buffer");
+    if (n < 2 || n > 1024) return fail(HRM_EINVAL, "grid edge out of range");
+    HRM_GUARD({
+        hrm_run_config cfg = config_or_default(cfg_in);
+        cudaStream_t s = (cudaStream_t)cfg.stream;
+        const size_t nvox = (size_t)n * n * n;
+        const size_t slots = nvox + 3u * hrm_specs::PHOTON_SPREAD;
+        DeviceArray<float> dm(nvox), da(nvox);
+        DeviceArray<uint8_t> dsp(nvox);
+        DeviceArray<uint64_t> dt(slots);
+        ck(cudaMemcpyAsync(dm.ptr, mu_s, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
+        ck(cudaMemcpyAsync(da.ptr, absorb, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
+        ck(cudaMemcpyAsync(dsp.ptr, split, nvox, cudaMemcpyHostToDevice, s), "medium upload");
+        int rc = photon_run(dm.ptr, da.ptr, dsp.ptr, n, seed, first, count, dt.ptr, &cfg, res);
+        if (rc != HRM_OK) return rc;
+        ck(cudaMemcpyAsync(tally, dt.ptr, slots * 8u, cudaMemcpyDeviceToHost, s), "tally download");
+        ck(cudaStreamSynchronize(s), "tally download");
+        return HRM_OK;
+    })
+}
+
+int hrm_bfs_run_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root,
+                       uint32_t* d_levels, const hrm_run_config* cfg, hrm_run_result* res) {
+    if (!d_rowptr || !d_col || !d_levels) return fail(HRM_EINVAL, "NULL buffer");
+    HRM_GUARD(return bfs_run(d_rowptr, d_col, nv, root, d_levels, cfg, res);)
+}
+
+int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32_t root, uint32_t* levels,
+                const hrm_run_config* cfg_in, hrm_run_result* res) {
+    if (!rowptr || !col || !levels) return fail(HRM_EINVAL, "NULL buffer");
+    if (nv == 0) return fail(HRM_EINVAL, "empty graph");
+    HRM_GUARD({
+        hrm_run_config cfg = config_or_default(cfg_in);
+        cudaStream_t s = (cudaStream_t)cfg.stream;
+        const size_t ne = rowptr[nv];
+        DeviceArray<uint32_t> drp((size_t)nv + 1), dcol(ne ? ne : 1), dlev(nv);
+        ck(cudaMemcpyAsync(drp.ptr, rowptr, ((size_t)nv + 1) * 4u, cudaMemcpyHostToDevice, s), "graph upload");
+        if (ne) ck(cudaMemcpyAsync(dcol.ptr, col, ne * 4u, cudaMemcpyHostToDevice, s), "graph upload");
+        int rc = bfs_run(drp.ptr, dcol.ptr, nv, root, dlev.ptr, &cfg, res);
+        if (rc != HRM_OK) return rc;
+        ck(cudaMemcpyAsync(levels, dlev.ptr, (size_t)nv * 4u, cudaMemcpyDeviceToHost, s), "levels download");
+        ck(cudaStreamSynchronize(s), "levels download");
         return HRM_OK;
     })
 }

@@ -1,0 +1,258 @@
+// photon.h — Monte Carlo optical photon random walk as a three-function async program.
+//
+// Workload (no counterpart file in Harmonize; the closest relative is the neutron example,
+// examples/cpp/example_neutron/program.cpp:11-44, whose float tallies are not
+// reproducible). Here every random number is a pure function of (photon id, step, phase)
+// and tallies are integers, so results do not depend on scheduling order:
+//  * an n^3 grid of unit voxels; voxel v has scattering coefficient mu_s[v], absorbed
+//    fraction absorb[v] and a split flag split[v];
+//  * photons start with weight 1 at the grid centre in an isotropic direction;
+//  * Move: sample a free path -ln(u)/mu_s; if it ends inside the voxel, move there and
+//    Collide; otherwise move to the voxel face, enter the neighbour (split x2 at half
+//    weight if the neighbour is flagged, re-sample the path there) or escape the grid;
+//  * Collide: deposit weight*absorb (Tally), keep the rest; below weight 1e-3 play Russian
+//    roulette (survive with probability 0.1 at ten times the weight); scatter isotropically;
+//  * Tally: add a 2^-32 fixed-point amount to a uint64 slot (atomic, order-independent).
+// Random numbers: Philox-4x32-10 with key = 64-bit photon id and counter =
+// (step, phase, seed_lo, seed_hi). Child ids are mix64 of (parent id, step, child index).
+// Floating point: every operation goes through hrm::f* (exactly rounded binary32), and
+// the logarithm is hrm::log_exact, so host and device results are bit-identical.
+#ifndef HRM_SPECS_PHOTON_H
+#define HRM_SPECS_PHOTON_H
+
+#include "../../../include/harmonize/spec_support.h"
+
+namespace hrm_specs {
+
+// Tally layout: [0, n^3) voxels, then PHOTON_SPREAD slots each for escaped weight,
+// roulette-killed weight and roulette-gained weight (spread to avoid one hot address).
+static const unsigned int PHOTON_SPREAD = 1024u;
+
+struct Photon {
+    float x, y, z;
+    float dx, dy, dz;
+    float w;
+    unsigned int id_lo, id_hi;
+    unsigned int step;
+    unsigned int voxel;
+};
+
+struct PhotonState {
+    const float* mu_s;
+    const float* absorb;
+    const unsigned char* split;
+    unsigned long long* tally;                      // n^3 + 3*PHOTON_SPREAD slots
+    util::iter::AtomicIter<unsigned int>* source;  // photon ids still to launch
+    unsigned int n;                                 // grid edge (voxels)
+    unsigned int seed_lo, seed_hi;
+    unsigned int leap;                              // photons per lane per make_work call
+    float load_limit;                               // stop launching above this load fraction
+};
+
+static const unsigned int PHASE_MOVE = 0u;
+static const unsigned int PHASE_ROULETTE = 1u;
+static const unsigned int PHASE_DIR = 2u;   // direction draws use phases 2 .. 2+15
+static const float WEIGHT_CUTOFF = 1.0e-3f;
+static const float ROULETTE_SURVIVAL = 0.1f;
+static const float ROULETTE_BOOST = 10.0f;
+
+HRM_HD HRM_FI hrm::U32x4 photon_rng(const PhotonState& s, unsigned int id_lo, unsigned int id_hi, unsigned int step,
+                                     unsigned int phase) {
+    hrm::U32x4 ctr = {step, phase, s.seed_lo, s.seed_hi};
+    return hrm::philox4x32_10(ctr, id_lo, id_hi);
+}
+
+HRM_HD HRM_FI unsigned long long to_fixed(float x) {
+    // x in [0, 1]; scaling by 2^32 is exact, conversion truncates on both sides.
+    return (unsigned long long)hrm::fmul(x, 4294967296.0f);
+}
+
+// Isotropic unit vector by Marsaglia's method (Ann. Math. Stat. 43, 1972): draw (u, v)
+// uniform in the unit disc, return (2u*sqrt(1-s), 2v*sqrt(1-s), 1-2s) with s = u^2+v^2.
+HRM_HD HRM_FI void isotropic(const PhotonState& st, unsigned int id_lo, unsigned int id_hi, unsigned int step,
+                             float& dx, float& dy, float& dz) {
+    for (unsigned int a = 0; a < 16u; a++) {
+        hrm::U32x4 r = photon_rng(st, id_lo, id_hi, step, PHASE_DIR + a);
+        unsigned int pair[4] = {r.x, r.y, r.z, r.w};
+        for (unsigned int q = 0; q < 4u; q += 2u) {
+            float u = hrm::u_pm1(pair[q]);
+            float v = hrm::u_pm1(pair[q + 1]);
+            float s = hrm::fadd(hrm::fmul(u, u), hrm::fmul(v, v));
+            if (s < 1.0f && s > 0.0f) {
+                float f = hrm::fmul(2.0f, hrm::fsqrt(hrm::fsub(1.0f, s)));
+                dx = hrm::fmul(u, f);
+                dy = hrm::fmul(v, f);
+                dz = hrm::fsub(1.0f, hrm::fmul(2.0f, s));
+                return;
+            }
+        }
+    }
+    dx = 0.0f;
+    dy = 0.0f;
+    dz = 1.0f;
+}
+
+struct PhotonMove;
+struct PhotonCollide;
+struct PhotonTally;
+
+struct PhotonTally {
+    using Type = void (*)(unsigned int, unsigned long long);
+    template <typename PROGRAM>
+    HRM_DEV static void eval(PROGRAM prog, unsigned int slot, unsigned long long amount) {
+        hrm::atomic_add_u64(&prog.device.tally[slot], amount);
+    }
+};
+
+// Distance along direction component d from coordinate x to the face of [lo, lo+1).
+HRM_HD HRM_FI float face_distance(float x, float d, unsigned int lo) {
+    if (d > 0.0f) {
+        float t = hrm::fdiv(hrm::fsub((float)(lo + 1u), x), d);
+        return t > 0.0f ? t : 0.0f;
+    }
+    if (d < 0.0f) {
+        float t = hrm::fdiv(hrm::fsub((float)lo, x), d);
+        return t > 0.0f ? t : 0.0f;
+    }
+    return 3.0e38f;
+}
+
+struct PhotonMove {
+    using Type = void (*)(Photon);
+    template <typename PROGRAM>
+    HRM_DEV static void eval(PROGRAM prog, Photon p) {
+        const PhotonState& s = prog.device;
+        const unsigned int n = s.n;
+        unsigned int ix = p.voxel % n, iy = (p.voxel / n) % n, iz = p.voxel / (n * n);
+        float mu = s.mu_s[p.voxel];
+        hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_MOVE);
+        float dist = hrm::fdiv(hrm::fsub(0.0f, hrm::log_exact(hrm::u01_open0(r.x))), mu);
+        float tx = face_distance(p.x, p.dx, ix);
+        float ty = face_distance(p.y, p.dy, iy);
+        float tz = face_distance(p.z, p.dz, iz);
+        unsigned int axis = 0;
+        float tb = tx;
+        if (ty < tb) { tb = ty; axis = 1; }
+        if (tz < tb) { tb = tz; axis = 2; }
+        p.step += 1u;
+        if (dist < tb) {
+            p.x = hrm::fadd(p.x, hrm::fmul(dist, p.dx));
+            p.y = hrm::fadd(p.y, hrm::fmul(dist, p.dy));
+            p.z = hrm::fadd(p.z, hrm::fmul(dist, p.dz));
+            prog.template async<PhotonCollide>(p);
+            return;
+        }
+        p.x = hrm::fadd(p.x, hrm::fmul(tb, p.dx));
+        p.y = hrm::fadd(p.y, hrm::fmul(tb, p.dy));
+        p.z = hrm::fadd(p.z, hrm::fmul(tb, p.dz));
+        // Land exactly on the face and step the voxel index along the crossing axis.
+        bool out = false;
+        if (axis == 0) {
+            if (p.dx > 0.0f) { p.x = (float)(ix + 1u); out = (ix + 1u == n); ix += 1u; }
+            else { p.x = (float)ix; out = (ix == 0u); ix -= 1u; }
+        } else if (axis == 1) {
+            if (p.dy > 0.0f) { p.y = (float)(iy + 1u); out = (iy + 1u == n); iy += 1u; }
+            else { p.y = (float)iy; out = (iy == 0u); iy -= 1u; }
+        } else {
+            if (p.dz > 0.0f) { p.z = (float)(iz + 1u); out = (iz + 1u == n); iz += 1u; }
+            else { p.z = (float)iz; out = (iz == 0u); iz -= 1u; }
+        }
+        if (out) {
+            prog.template async<PhotonTally>(n * n * n + (p.id_lo & (PHOTON_SPREAD - 1u)), to_fixed(p.w));
+            return;
+        }
+        p.voxel = ix + n * (iy + n * iz);
+        if (s.split[p.voxel]) {
+            p.w = hrm::fmul(p.w, 0.5f);
+            unsigned long long id = ((unsigned long long)p.id_hi << 32) | p.id_lo;
+            for (unsigned int c = 0; c < 2u; c++) {
+                unsigned long long cid = hrm::mix64(id ^ (((unsigned long long)p.step << 1) | c) * 0x9E3779B97F4A7C15ull);
+                Photon q = p;
+                q.id_lo = (unsigned int)cid;
+                q.id_hi = (unsigned int)(cid >> 32);
+                prog.template async<PhotonMove>(q);
+            }
+            return;
+        }
+        prog.template async<PhotonMove>(p);
+    }
+};
+
+struct PhotonCollide {
+    using Type = void (*)(Photon);
+    template <typename PROGRAM>
+    HRM_DEV static void eval(PROGRAM prog, Photon p) {
+        const PhotonState& s = prog.device;
+        const unsigned int n = s.n;
+        float dep = hrm::fmul(p.w, s.absorb[p.voxel]);
+        p.w = hrm::fsub(p.w, dep);
+        prog.template async<PhotonTally>(p.voxel, to_fixed(dep));
+        if (p.w < WEIGHT_CUTOFF) {
+            hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_ROULETTE);
+            unsigned int spread = p.id_lo & (PHOTON_SPREAD - 1u);
+            if (hrm::u01_open0(r.x) <= ROULETTE_SURVIVAL) {
+                float boosted = hrm::fmul(p.w, ROULETTE_BOOST);
+                prog.template async<PhotonTally>(n * n * n + 2u * PHOTON_SPREAD + spread,
+                                                 to_fixed(hrm::fsub(boosted, p.w)));
+                p.w = boosted;
+            } else {
+                prog.template async<PhotonTally>(n * n * n + PHOTON_SPREAD + spread, to_fixed(p.w));
+                return;
+            }
+        }
+        isotropic(s, p.id_lo, p.id_hi, p.step, p.dx, p.dy, p.dz);
+        p.step += 1u;
+        prog.template async<PhotonMove>(p);
+    }
+};
+
+// A photon launched from the grid centre (a voxel corner when n is even): it starts in
+// the voxel its direction points into.
+HRM_HD HRM_FI Photon photon_source(const PhotonState& s, unsigned int id) {
+    Photon p;
+    const unsigned int h = s.n / 2u;
+    p.x = (float)h;
+    p.y = (float)h;
+    p.z = (float)h;
+    p.id_lo = id;
+    p.id_hi = 0u;
+    p.step = 0u;
+    p.w = 1.0f;
+    isotropic(s, p.id_lo, p.id_hi, 0u, p.dx, p.dy, p.dz);
+    unsigned int ix = p.dx >= 0.0f ? h : h - 1u;
+    unsigned int iy = p.dy >= 0.0f ? h : h - 1u;
+    unsigned int iz = p.dz >= 0.0f ? h : h - 1u;
+    p.voxel = ix + s.n * (iy + s.n * iz);
+    p.step = 1u;
+    return p;
+}
+
+template <size_t RING = 2, size_t TEAMS = 4>
+struct PhotonSpec {
+    typedef OpUnion<PhotonMove, PhotonCollide, PhotonTally> OpSet;
+    typedef PhotonState DeviceState;
+
+    static const size_t STASH_SIZE = 8;
+    static const size_t FRAME_SIZE = 16069;
+    static const size_t POOL_SIZE = 16069;
+    static const size_t RING_LINKS = RING;
+    static const size_t TEAMS_PER_CTA = TEAMS;
+
+    template <typename PROGRAM>
+    HRM_DEV static bool make_work(PROGRAM prog) {
+        // EventProgram: stop launching while the move buffer is loaded (load_fraction is NaN
+        // under AsyncProgram, so the comparison is false there).
+        float load = prog.template load_fraction<PhotonMove>();
+        if (load > prog.device.load_limit) return false;
+        util::iter::Iter<unsigned int> it = prog.device.source->leap(prog.device.leap);
+        unsigned int id;
+        while (it.step(id)) {
+            prog.template async<PhotonMove>(photon_source(prog.device, id));
+        }
+        return !prog.device.source->done();
+    }
+};
+
+}  // namespace hrm_specs
+
+#endif

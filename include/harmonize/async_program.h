@@ -632,6 +632,7 @@ class AsyncProgram {
         bool counted_idle = false;
         unsigned int backoff = 32;
         unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_spill = 0, n_fill = 0, n_mw = 0, n_idle = 0;
+        unsigned long long fn_evals = 0;  // lane f counts the evaluations of function f
         bool quiescent = false;
 
         for (unsigned int cycle = 0; cycle < cycle_count; cycle++) {
@@ -664,8 +665,13 @@ class AsyncProgram {
                     unsigned int took = fill_fn<0>(ff);
                     n_fill += took;
                     if (took > 0) continue;
-                }
-                if (can_make_work) {
+                    // Another team won the race for that work. Never make new work while
+                    // the arena holds a backlog: run what is local, or look again.
+                    if (bc == 0) {
+                        __nanosleep(64);
+                        continue;
+                    }
+                } else if (can_make_work) {
                     if (counted_idle) {
                         if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
                         counted_idle = false;
@@ -708,6 +714,7 @@ class AsyncProgram {
             n_evals += k;
             n_batches += 1;
             n_full += (k == 32u);
+            if (lane == bf) fn_evals += k;
         }
 
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
@@ -718,6 +725,7 @@ class AsyncProgram {
             unsigned int cf = g.count[f];
             if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
         }
+        if (lane < FN && fn_evals != 0) atomicAdd(&_dev_ctx.stats[hrm_rt::STAT_FN_EVALS + lane], fn_evals);
         if (lane == 0) {
             if (can_make_work) atomicOr(&ctl->flags, EARLY_HALT_FLAG);
             for (unsigned int f = 0; f < FN; f++) {
@@ -773,13 +781,26 @@ class AsyncProgram {
     // ===================================================================================
     // Host launch helpers used by init<P> and exec<P>.
     // ===================================================================================
+    // Team stashes live in dynamic shared memory: TEAMS_PER_CTA contexts, then as many
+    // GroupStates, each rounded up to 16 bytes.
+    static constexpr size_t align16(size_t x) { return (x + 15u) & ~(size_t)15u; }
+    static const size_t CTX_BYTES = align16(sizeof(GroupContext));
+    static const size_t STATE_BYTES = align16(sizeof(GroupState));
+    static const size_t SMEM_BYTES = TEAMS_PER_CTA * (CTX_BYTES + STATE_BYTES);
+    static_assert(SMEM_BYTES <= 227u * 1024u, "team stashes exceed 227 KB of shared memory per CTA");
+
+    // Opts the exec kernel into more than 48 KB of dynamic shared memory (once per device)
+    // and returns how many of its CTAs can be resident at once.
     static unsigned int resident_ctas() {
         static int cached_dev = -1;
         static unsigned int cached = 0;
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev != cached_dev) {
-            cached = hrm_rt::max_resident_ctas(hrm_rt::async_exec_kernel<ProgramType>, (int)CTA_THREADS, 0);
+            util::host::auto_throw(cudaFuncSetAttribute(hrm_rt::async_exec_kernel<ProgramType>,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)SMEM_BYTES));
+            cached = hrm_rt::max_resident_ctas(hrm_rt::async_exec_kernel<ProgramType>, (int)CTA_THREADS, SMEM_BYTES);
             cached_dev = dev;
         }
         return cached;
@@ -803,7 +824,8 @@ class AsyncProgram {
         unsigned int cycles = cycle_count > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned int)cycle_count;
         DeviceContext ctx = inst.to_context();
         hrm_rt::async_prep_kernel<ProgramType><<<1, 32, 0, stream>>>(ctx, ctas * TEAMS_PER_CTA);
-        hrm_rt::async_exec_kernel<ProgramType><<<ctas, CTA_THREADS, 0, stream>>>(ctx, inst.device_state, cycles);
+        hrm_rt::async_exec_kernel<ProgramType><<<ctas, CTA_THREADS, SMEM_BYTES, stream>>>(ctx, inst.device_state,
+                                                                                           cycles);
     }
 };
 
@@ -830,12 +852,14 @@ __global__ void async_prep_kernel(typename PROG::DeviceContext ctx, unsigned int
 template <typename PROG>
 __global__ void __launch_bounds__(PROG::CTA_THREADS, PROG::MIN_CTAS_PER_SM)
     async_exec_kernel(typename PROG::DeviceContext ctx, typename PROG::DeviceState device, unsigned int cycles) {
-    __shared__ typename PROG::GroupContext grp_ctx[PROG::TEAMS_PER_CTA];
-    __shared__ typename PROG::GroupState grp_state[PROG::TEAMS_PER_CTA];
+    extern __shared__ __align__(16) unsigned char hrm_team_smem[];
     const unsigned int team = threadIdx.x >> 5;
+    auto* grp_ctx = reinterpret_cast<typename PROG::GroupContext*>(hrm_team_smem + team * PROG::CTX_BYTES);
+    auto* grp_state = reinterpret_cast<typename PROG::GroupState*>(
+        hrm_team_smem + PROG::TEAMS_PER_CTA * PROG::CTX_BYTES + team * PROG::STATE_BYTES);
     typename PROG::ThreadContext thd_ctx;
     typename PROG::ThreadState thd_state;
-    PROG prog(ctx, grp_ctx[team], thd_ctx, device, grp_state[team], thd_state);
+    PROG prog(ctx, *grp_ctx, thd_ctx, device, *grp_state, thd_state);
     prog.exec(cycles);
 }
 

@@ -371,6 +371,7 @@ class EventProgram {
         hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
         if (chunk == 0) chunk = 1;
         unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_mw = 0, n_gen = 0;
+        unsigned long long fn_evals = 0;  // lane f counts the evaluations of function f
 
         for (unsigned int gen = 0; gen < max_generations; gen++) {
             // This generation's schedule: lane f holds function f's first tile and count.
@@ -399,6 +400,7 @@ class EventProgram {
                     n_evals += k;
                     n_batches += 1;
                     n_full += (k == 32u);
+                    if (lane == f) fn_evals += k;
                 }
             }
             // All inputs claimed: make work until told to stop or an output is half full.
@@ -428,6 +430,7 @@ class EventProgram {
         }
 
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
+        if (lane < FN && fn_evals != 0) atomicAdd(&_dev_ctx.stats[hrm_rt::STAT_FN_EVALS + lane], fn_evals);
         if (lane == 0) {
             unsigned long long* st = _dev_ctx.stats;
             atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);

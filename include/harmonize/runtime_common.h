@@ -172,7 +172,8 @@ enum StatIndex : unsigned int {
     STAT_MAKE_WORK = 5,   // make_work calls (per team)
     STAT_IDLE_POLLS = 6,  // polls made while idle
     STAT_GENERATIONS = 7, // EventProgram generations
-    STAT_COUNT = 8
+    STAT_FN_EVALS = 8,    // STAT_FN_EVALS + f: promises of function f evaluated (f < 16)
+    STAT_COUNT = 24
 };
 
 // ---------------------------------------------------------------------------------------

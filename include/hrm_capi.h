@@ -61,7 +61,8 @@ extern "C" {
 #define HRM_STAT_MAKE_WORK 5
 #define HRM_STAT_IDLE_POLLS 6
 #define HRM_STAT_GENERATIONS 7
-#define HRM_STAT_COUNT 8
+#define HRM_STAT_FN_EVALS 8   /* HRM_STAT_FN_EVALS + f: evaluations of async function f (f < 16) */
+#define HRM_STAT_COUNT 24
 
 typedef struct hrm_program hrm_program; /* opaque: one program instance on one device */
 
@@ -74,7 +75,17 @@ typedef struct hrm_run_config {
     size_t arena;              /* AsyncProgram arena links / EventProgram io_size; 0 = default */
     size_t max_execs;          /* exec calls before giving up with HRM_EINCOMPLETE; 0 = 4096 */
     void* stream;              /* cudaStream_t, NULL = default stream */
+    int variant;               /* compiled tuning variant (see HRM_VARIANT_*), 0 = default */
 } hrm_run_config;
+
+/* Compiled tuning variants: shared-memory ring per async function (in 32-promise links)
+ * and 32-lane teams per CTA. EventProgram uses only the team count. */
+#define HRM_VARIANT_R2_T4 0
+#define HRM_VARIANT_R4_T4 1
+#define HRM_VARIANT_R4_T2 2
+#define HRM_VARIANT_R8_T2 3
+#define HRM_VARIANT_R2_T8 4
+#define HRM_VARIANT_COUNT 5
 
 /* What a whole run reports back. */
 typedef struct hrm_run_result {
@@ -96,6 +107,9 @@ int hrm_device_sync(void);
  *   flag returns HRM_EDEVICE). */
 int hrm_program_create(int spec, int program_type, size_t arena_or_io, const void* device_state,
                        size_t state_size, hrm_program** out);
+/* Same, choosing a compiled tuning variant (HRM_VARIANT_*). */
+int hrm_program_create_variant(int spec, int program_type, int variant, size_t arena_or_io,
+                               const void* device_state, size_t state_size, hrm_program** out);
 int hrm_program_destroy(hrm_program* prog);
 int hrm_program_init(hrm_program* prog, size_t groups, void* stream);
 int hrm_program_exec(hrm_program* prog, size_t groups, size_t cycles_or_chunk, void* stream);
@@ -118,6 +132,28 @@ typedef struct hrm_collatz_state {
     uint32_t leap;             /* start values per lane per make_work call (0 = 1) */
 } hrm_collatz_state;
 
+typedef struct hrm_photon_state {
+    const float* mu_s;         /* device: scattering coefficient per voxel (n^3) */
+    const float* absorb;       /* device: absorbed fraction per collision per voxel */
+    const uint8_t* split;      /* device: 1 = photons entering the voxel split in two */
+    uint64_t* tally;           /* device: n^3 voxel tallies + 3*1024 escape/kill/gain slots,
+                                  2^-32 fixed point */
+    void* source;              /* device pointer to an AtomicIter<uint32> over photon ids */
+    uint32_t n;                /* grid edge in voxels (even) */
+    uint32_t seed_lo, seed_hi; /* Philox counter words 2 and 3 */
+    uint32_t leap;             /* photons per lane per make_work call (0 = 1) */
+    float load_limit;          /* EventProgram: launch no photons above this move-buffer load */
+} hrm_photon_state;
+
+typedef struct hrm_bfs_state {
+    const uint32_t* rowptr;    /* device CSR row offsets (nv + 1) */
+    const uint32_t* col;       /* device CSR targets */
+    uint32_t* levels;          /* device, nv entries, pre-filled with 0xFFFFFFFF */
+    void* roots;               /* device pointer to an AtomicIter<uint32> over [0, 1) */
+    uint32_t root;
+    uint32_t nv;
+} hrm_bfs_state;
+
 /* ---- whole runs (host buffers in and out) --------------------------------------------- */
 
 /* Collatz stopping times of n = start .. start+count-1 into out_steps[count] (host). */
@@ -126,6 +162,32 @@ int hrm_collatz_run(uint32_t start, uint32_t count, uint32_t* out_steps, const h
 /* Same, with a device output buffer (no host copies). */
 int hrm_collatz_run_device(uint32_t start, uint32_t count, uint32_t* d_out_steps, const hrm_run_config* cfg,
                            hrm_run_result* res);
+
+/* Photon walk of photons [first, first+count) over an n^3 medium (host arrays of n^3);
+ * tally receives n^3 + 3*1024 uint64 slots (voxels, then escaped, roulette-killed and
+ * roulette-gained weight, each spread over 1024 slots), in units of 2^-32. */
+int hrm_photon_run(const float* mu_s, const float* absorb, const uint8_t* split, uint32_t n, uint64_t seed,
+                   uint32_t first, uint32_t count, uint64_t* tally, const hrm_run_config* cfg,
+                   hrm_run_result* res);
+int hrm_photon_run_device(const float* d_mu_s, const float* d_absorb, const uint8_t* d_split, uint32_t n,
+                          uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally,
+                          const hrm_run_config* cfg, hrm_run_result* res);
+
+/* Breadth-first levels from `root` over a CSR graph (host arrays); unreached = 0xFFFFFFFF. */
+int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32_t root, uint32_t* levels,
+                const hrm_run_config* cfg, hrm_run_result* res);
+int hrm_bfs_run_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root,
+                       uint32_t* d_levels, const hrm_run_config* cfg, hrm_run_result* res);
+
+/* ---- seeded synthetic inputs (host) ---------------------------------------------------- */
+
+/* R-MAT graph with 2^scale vertices and edge_factor * 2^scale edges, quadrant
+ * probabilities (a, b, c, 1-a-b-c), as CSR sorted by (source, target):
+ * rowptr[2^scale + 1], col[edge_factor * 2^scale]. Returns 0, or 1 on bad arguments. */
+int hrm_rmat_csr(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                 uint32_t* rowptr, uint32_t* col);
+/* Photon medium: mu_s ~ lognormal(0, 0.5), absorb ~ U[0.02, 0.2], split with p = 0.1. */
+int hrm_photon_medium(uint32_t n, uint64_t seed, float* mu_s, float* absorb, uint8_t* split);
 
 #ifdef __cplusplus
 }

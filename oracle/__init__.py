@@ -1,18 +1,21 @@
 """CPU oracle for the B200 Harmonize runtime — TEST INFRASTRUCTURE ONLY.
 
-Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
-may import this package. The product (``harmonize_b200``) never imports, links or runs
-anything here; its GPU path fails loudly when its CUDA library is missing.
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of
+``bench.py`` may import this package. The product (``harmonize_b200``) never imports, links
+or runs anything here; its GPU path fails loudly when its CUDA library is missing.
 
 Contents:
-  * plain-C restatements of the reference's checkers and of the workloads' algorithms
-    (``collatz.c``, ``bfs.c``, ``photon.c``), each citing the reference file it follows;
+  * plain-C restatements of the reference's checker and of the workloads' algorithms
+    (``collatz.c`` after examples/cpp/collaz/collaz_hrm.cpp:157-168, ``bfs.c``,
+    ``photon.c``);
   * host executors (``host_exec.cpp``) that run the very same spec sources as the GPU
     runtime, serially and with OpenMP — Harmonize itself has no CPU executor;
-  * ``build.py``, which compiles the above into ``oracle/_build/liboracle.so`` and, when
-    the reference tree is present, the reference CUDA build into ``oracle/_ref``.
+  * ``build.py``, which compiles the above into ``oracle/_build/liboracle.so``;
+    ``ref_build.py`` builds the reference CUDA build of the same specs into ``oracle/_ref``.
 
-Parity pins: the Collatz restatement is checked against known stopping times and against
-the reference runtime's own outputs committed under ``tests/golden``.
+Parity pins: the Collatz restatement is checked against known stopping times and the
+reference runtime's own outputs (``tests/golden``); the photon and BFS restatements agree
+bit for bit with the host executors of the spec sources and with the reference runtime.
 """
-from .lib import load, collatz_range  # noqa: F401
+from .lib import (load, max_threads, collatz_range, exec_collatz, bfs, exec_bfs,  # noqa: F401
+                  photon_walk, exec_photon, philox, log, PHOTON_SPREAD)

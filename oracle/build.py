@@ -12,8 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
 
-C_SOURCES = ["collatz.c"]
-CXX_SOURCES = []
+C_SOURCES = ["collatz.c", "bfs.c", "photon.c"]
+CXX_SOURCES = ["host_exec.cpp"]
+SPEC_DIR = os.path.join(HERE, "..", "harmonize_b200", "csrc", "specs")
 
 
 def _newer(target, sources):
@@ -26,7 +27,9 @@ def _newer(target, sources):
 def build(force=False, quiet=True):
     os.makedirs(BUILD, exist_ok=True)
     srcs = [os.path.join(HERE, s) for s in C_SOURCES + CXX_SOURCES]
-    deps = srcs + [os.path.join(HERE, "host_api.h")] if os.path.exists(os.path.join(HERE, "host_api.h")) else srcs
+    deps = srcs + [os.path.join(HERE, "host_api.h"),
+                   os.path.join(HERE, "..", "include", "harmonize", "spec_support.h")]
+    deps += [os.path.join(SPEC_DIR, f) for f in os.listdir(SPEC_DIR) if f.endswith(".h")]
     if not force and not _newer(LIB, deps):
         return LIB
     objs = []

@@ -7,22 +7,110 @@ import numpy as np
 from . import build as _build
 
 _lib = None
+PHOTON_SPREAD = 1024
 
 
 def load():
     global _lib
     if _lib is None:
         path = _build.build()
-        _lib = ctypes.CDLL(path)
-        _lib.oracle_collatz_steps.restype = ctypes.c_uint32
-        _lib.oracle_collatz_steps.argtypes = [ctypes.c_uint64]
-        _lib.oracle_collatz_range.restype = None
-        _lib.oracle_collatz_range.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
+        L = ctypes.CDLL(path)
+        vp, u32, u64, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        sig = {
+            "oracle_collatz_steps": (u32, [u64]),
+            "oracle_collatz_range": (None, [u32, u32, vp]),
+            "oracle_bfs": (u32, [vp, vp, u32, u32, vp]),
+            "oracle_photon_walk": (None, [vp, vp, vp, u32, u32, u32, u32, u32, vp, vp]),
+            "oracle_philox4x32_10": (None, [vp, vp, vp]),
+            "oracle_log": (ctypes.c_float, [ctypes.c_float]),
+            "oracle_max_threads": (i32, []),
+            "oracle_exec_collatz": (None, [u32, u32, vp, i32, vp]),
+            "oracle_exec_photon": (None, [vp, vp, vp, u32, u32, u32, u32, u32, vp, i32, vp]),
+            "oracle_exec_bfs": (None, [vp, vp, u32, u32, vp, i32, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
     return _lib
 
 
+def max_threads():
+    return load().oracle_max_threads()
+
+
 def collatz_range(start, count):
-    """Stopping times of start .. start+count-1 (uint32 array)."""
+    """Stopping times of start .. start+count-1 (uint32), plain restatement."""
     out = np.zeros(count, dtype=np.uint32)
     load().oracle_collatz_range(start, count, out.ctypes.data)
     return out
+
+
+def exec_collatz(start, count, threads=0):
+    """Same spec source as the GPU runtime, host executor. Returns (steps, calls[2])."""
+    out = np.zeros(count, dtype=np.uint32)
+    calls = np.zeros(2, dtype=np.uint64)
+    load().oracle_exec_collatz(start, count, out.ctypes.data, threads, calls.ctypes.data)
+    return out, calls
+
+
+def bfs(rowptr, col, root):
+    """Serial textbook BFS levels (uint32, unreached = 0xFFFFFFFF)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    nv = len(rowptr) - 1
+    levels = np.empty(nv, dtype=np.uint32)
+    load().oracle_bfs(rowptr.ctypes.data, col.ctypes.data, nv, root, levels.ctypes.data)
+    return levels
+
+
+def exec_bfs(rowptr, col, root, threads=0):
+    """Same BFS spec as the GPU runtime on the host executor. Returns (levels, calls[2])."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    nv = len(rowptr) - 1
+    levels = np.full(nv, 0xFFFFFFFF, dtype=np.uint32)
+    calls = np.zeros(2, dtype=np.uint64)
+    load().oracle_exec_bfs(rowptr.ctypes.data, col.ctypes.data, nv, root, levels.ctypes.data, threads,
+                           calls.ctypes.data)
+    return levels, calls
+
+
+def _medium_args(mu_s, absorb, split):
+    mu_s = np.ascontiguousarray(mu_s, dtype=np.float32)
+    absorb = np.ascontiguousarray(absorb, dtype=np.float32)
+    split = np.ascontiguousarray(split, dtype=np.uint8)
+    return mu_s, absorb, split
+
+
+def photon_walk(mu_s, absorb, split, n, seed, first, count):
+    """Plain-C restatement of the photon walk. Returns (tally uint64[n^3+3*1024], calls[3])."""
+    mu_s, absorb, split = _medium_args(mu_s, absorb, split)
+    tally = np.zeros(n ** 3 + 3 * PHOTON_SPREAD, dtype=np.uint64)
+    calls = np.zeros(3, dtype=np.uint64)
+    load().oracle_photon_walk(mu_s.ctypes.data, absorb.ctypes.data, split.ctypes.data, n, seed & 0xFFFFFFFF,
+                              seed >> 32, first, count, tally.ctypes.data, calls.ctypes.data)
+    return tally, calls
+
+
+def exec_photon(mu_s, absorb, split, n, seed, first, count, threads=0):
+    """Photon spec on the host executor. Returns (tally, calls[3] = move, collide, tally)."""
+    mu_s, absorb, split = _medium_args(mu_s, absorb, split)
+    tally = np.zeros(n ** 3 + 3 * PHOTON_SPREAD, dtype=np.uint64)
+    calls = np.zeros(3, dtype=np.uint64)
+    load().oracle_exec_photon(mu_s.ctypes.data, absorb.ctypes.data, split.ctypes.data, n, seed & 0xFFFFFFFF,
+                              seed >> 32, first, count, tally.ctypes.data, threads, calls.ctypes.data)
+    return tally, calls
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    load().oracle_philox4x32_10(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return out
+
+
+def log(x):
+    return load().oracle_log(x)

@@ -1,0 +1,39 @@
+"""Photon walk on the GPU runtime against the CPU oracle: bit-exact uint64 fixed-point tallies
+and identical per-run call counts (every call is a pure function of photon id and step)."""
+import numpy as np
+import pytest
+
+import oracle
+
+
+@pytest.fixture(scope="module")
+def medium16(hrm):
+    return hrm.photon_medium(16, 11)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("program", ["async", "event"])
+@pytest.mark.parametrize("first,count", [(0, 1), (0, 700), (123456, 3000)])
+def test_photon_matches_oracle(hrm, medium16, program, first, count):
+    mu, ab, sp = medium16
+    tally, res = hrm.photon_walk(mu, ab, sp, 16, 0xC0FFEE, first, count, program=program)
+    ref, calls = oracle.photon_walk(mu, ab, sp, 16, 0xC0FFEE, first, count)
+    assert np.array_equal(tally, ref)
+    assert res["evals"] == int(calls.sum())
+
+
+@pytest.mark.gpu
+def test_photon_async_equals_event_large_grid(hrm):
+    mu, ab, sp = hrm.photon_medium(64, 5)
+    a, ra = hrm.photon_walk(mu, ab, sp, 64, 17, 0, 20000, program="async")
+    e, re = hrm.photon_walk(mu, ab, sp, 64, 17, 0, 20000, program="event")
+    ref, calls = oracle.photon_walk(mu, ab, sp, 64, 17, 0, 20000)
+    assert np.array_equal(a, ref) and np.array_equal(e, ref)
+    assert ra["evals"] == re["evals"] == int(calls.sum())
+
+
+@pytest.mark.gpu
+def test_photon_zero_photons(hrm, medium16):
+    mu, ab, sp = medium16
+    tally, res = hrm.photon_walk(mu, ab, sp, 16, 1, 0, 0)
+    assert not tally.any() and res["evals"] == 0
