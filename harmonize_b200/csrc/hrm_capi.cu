@@ -9,6 +9,7 @@
 #include "specs/collatz.h"
 #include "specs/photon.h"
 
+#include <chrono>
 #include <mutex>
 #include <string>
 
@@ -474,3 +475,170 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
 }
 
 }  // extern "C"
+
+// =======================================================================================
+// hrm_collatz_run_device_noalloc: a Collatz whole run that allocates no device memory.
+//
+// Why it exists: some callers cannot call cudaMalloc at the moment they want to run the
+// program. Examples: code recording work into a CUDA stream capture that must not gain
+// allocation nodes, plug-in hosts that hand out only buffers registered ahead of time,
+// and services that forbid allocation after start-up to keep their memory use fixed. Every
+// other entry point here builds a program instance with cudaMalloc (arena, queues, control
+// block); this one runs the same AsyncProgram<CollatzSpec<2,4>> kernels over a scratch
+// area compiled into the library.
+//
+// The scratch area is the file-scope array g_noalloc_scratch (about 2.2 MiB); every GPU
+// that loads this library holds it until the process exits. It caps the runtime arena at
+// HRM_NOALLOC_MAX_ARENA_LINKS links of 32 promises: larger requests are rejected, and a run
+// whose promises in flight outgrow it stops with ARENA_EXHAUSTED (HRM_EDEVICE).
+//
+// In host code the name g_noalloc_scratch is a host-side stand-in, not a device address:
+// a kernel handed it would fault or, where the GPU can reach host memory, silently use the
+// wrong memory. So the first call on each device, with that device current, looks up the
+// device address once with cudaGetSymbolAddress and keeps it; make that first call before
+// any stream capture starts.
+//
+// All calls share the one array, which keeps the previous call's contents; each call
+// rewrites everything the run needs initialised. Calls that overlap on the GPU (several host
+// threads, or several streams) use the same scratch and race: serialise them.
+// =======================================================================================
+namespace {
+
+using NoAllocProgram = AsyncProgram<hrm_specs::CollatzSpec<2, 4>>;
+
+constexpr size_t NA_LINKS = HRM_NOALLOC_MAX_ARENA_LINKS;  // a power of two: also the ring capacity
+static_assert((NA_LINKS & (NA_LINKS - 1)) == 0, "no-allocation arena must be a power of two");
+constexpr size_t NA_FN = NoAllocProgram::FN;
+constexpr size_t NA_LINK_WORDS = NoAllocProgram::LINK_WORDS;
+
+// Layout of the scratch area: byte offsets, each 256-byte aligned.
+constexpr size_t na_align(size_t x) { return (x + 255u) & ~(size_t)255u; }
+constexpr size_t NA_OFF_CONTROL = 0;
+constexpr size_t NA_OFF_HEADS = na_align(NA_OFF_CONTROL + sizeof(hrm_rt::RuntimeControl));
+constexpr size_t NA_OFF_STATS = na_align(NA_OFF_HEADS + sizeof(hrm_rt::RingHead) * (NA_FN + 1));
+constexpr size_t NA_OFF_ITER = na_align(NA_OFF_STATS + sizeof(unsigned long long) * hrm_rt::STAT_COUNT);
+constexpr size_t NA_OFF_SLOTS = na_align(NA_OFF_ITER + sizeof(util::iter::AtomicIter<unsigned int>));
+constexpr size_t NA_OFF_META = na_align(NA_OFF_SLOTS + sizeof(unsigned long long) * (NA_FN + 1) * NA_LINKS);
+constexpr size_t NA_OFF_WORDS = na_align(NA_OFF_META + sizeof(unsigned int) * 2u * NA_LINKS);
+constexpr size_t NA_SCRATCH_BYTES = na_align(NA_OFF_WORDS + sizeof(unsigned int) * NA_LINK_WORDS * 32u * NA_LINKS);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch, looked up once per device.
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex g_na_mutex;
+unsigned char* g_na_address[NA_MAX_DEVICES] = {};
+
+unsigned char* noalloc_scratch_address() {
+    int dev = -1;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= NA_MAX_DEVICES) throw std::invalid_argument("device index beyond the supported 64");
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (g_na_address[dev] == nullptr) {
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-allocation scratch)");
+        if (p == nullptr) throw std::runtime_error("cudaGetSymbolAddress returned NULL for the scratch area");
+        g_na_address[dev] = (unsigned char*)p;
+    }
+    return g_na_address[dev];
+}
+
+// Sets the start-value iterator that lives in the scratch area.
+__global__ void noalloc_iterator_kernel(util::iter::AtomicIter<unsigned int>* it, unsigned int start,
+                                        unsigned int limit) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        it->value = start;
+        it->limit = limit;
+    }
+}
+
+int collatz_run_noalloc(uint32_t start, uint32_t count, uint32_t* d_out, const hrm_run_config* cfg_in,
+                        hrm_run_result* res) {
+    hrm_run_config cfg = config_or_default(cfg_in);
+    if ((uint64_t)start + count > 0xFFFFFFFFull) return fail(HRM_EINVAL, "start + count exceeds 2^32");
+    if (cfg.program_type != HRM_ASYNC) return fail(HRM_EINVAL, "the no-allocation entry point runs AsyncProgram only");
+    if (cfg.variant != 0) return fail(HRM_EINVAL, "the no-allocation entry point runs tuning variant 0 only");
+    size_t arena = cfg.arena ? cfg.arena : NA_LINKS;
+    if (arena > NA_LINKS) {
+        return fail(HRM_EINVAL, "requested arena of " + std::to_string(arena) +
+                                    " links exceeds the no-allocation maximum of " + std::to_string(NA_LINKS) +
+                                    " links");
+    }
+    unsigned char* base = noalloc_scratch_address();
+    cudaStream_t s = (cudaStream_t)cfg.stream;
+
+    NoAllocProgram::DeviceContext ctx;
+    ctx.ctl = (hrm_rt::RuntimeControl*)(base + NA_OFF_CONTROL);
+    ctx.rings.heads = (hrm_rt::RingHead*)(base + NA_OFF_HEADS);
+    ctx.rings.slots = (unsigned long long*)(base + NA_OFF_SLOTS);
+    ctx.rings.mask = (unsigned int)NA_LINKS - 1u;
+    ctx.link_words = (unsigned int*)(base + NA_OFF_WORDS);
+    ctx.link_meta = (unsigned int*)(base + NA_OFF_META);
+    ctx.stats = (unsigned long long*)(base + NA_OFF_STATS);
+    ctx.arena_links = (unsigned int)arena;
+    auto* it = (util::iter::AtomicIter<unsigned int>*)(base + NA_OFF_ITER);
+
+    hrm_specs::CollatzState st;
+    st.start = start;
+    st.limit = start + count;
+    st.output = d_out;
+    st.iterator = it;
+    st.leap = 1;
+
+    size_t groups = cfg.groups ? cfg.groups : (size_t)1 << 30;
+    size_t cycles = cfg.cycles ? cfg.cycles : ((size_t)1 << 24);
+    size_t max_execs = cfg.max_execs ? cfg.max_execs : 4096;
+    unsigned int ctas = NoAllocProgram::ctas_for(groups);
+    unsigned int cyc = cycles > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned int)cycles;
+
+    auto t0 = std::chrono::steady_clock::now();
+    // The init kernel rewrites every ring slot, ring head, control word and statistic, so
+    // nothing the previous call left behind reaches this run.
+    noalloc_iterator_kernel<<<1, 32, 0, s>>>(it, start, start + count);
+    ck(cudaGetLastError(), "iterator launch");
+    hrm_rt::async_init_kernel<NoAllocProgram><<<148, 256, 0, s>>>(ctx);
+    ck(cudaGetLastError(), "init launch");
+    size_t execs = 0;
+    bool done = false;
+    unsigned int flags = 0;
+    while (execs < max_execs) {
+        hrm_rt::async_prep_kernel<NoAllocProgram><<<1, 32, 0, s>>>(ctx, ctas * NoAllocProgram::TEAMS_PER_CTA);
+        hrm_rt::async_exec_kernel<NoAllocProgram>
+            <<<ctas, NoAllocProgram::CTA_THREADS, NoAllocProgram::SMEM_BYTES, s>>>(ctx, st, cyc);
+        ck(cudaGetLastError(), "exec launch");
+        execs++;
+        ck(cudaMemcpyAsync(&flags, &ctx.ctl->flags, sizeof(flags), cudaMemcpyDeviceToHost, s), "flags read");
+        ck(cudaStreamSynchronize(s), "exec");
+        if (flags & hrm_rt::ERROR_MASK) break;
+        if (flags & hrm_rt::COMPLETION_FLAG) {
+            done = true;
+            break;
+        }
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (res) {
+        unsigned long long st_host[hrm_rt::STAT_COUNT];
+        ck(cudaMemcpy(st_host, ctx.stats, sizeof(st_host), cudaMemcpyDeviceToHost), "stats read");
+        res->flags = flags;
+        res->execs = (uint32_t)execs;
+        for (int i = 0; i < HRM_STAT_COUNT; i++) res->stats[i] = st_host[i];
+        res->device_ms = (float)std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    if (flags & hrm_rt::ERROR_MASK) {
+        try {
+            hrm_rt::throw_flags(flags);
+        } catch (std::runtime_error& e) {
+            return fail(HRM_EDEVICE, e.what());
+        }
+    }
+    if (!done) return fail(HRM_EINCOMPLETE, "run did not complete within max_execs exec calls");
+    return HRM_OK;
+}
+
+}  // namespace
+
+extern "C" int hrm_collatz_run_device_noalloc(uint32_t start, uint32_t count, uint32_t* d_out_steps,
+                                              const hrm_run_config* cfg, hrm_run_result* res) {
+    if (d_out_steps == nullptr && count != 0) return fail(HRM_EINVAL, "output is NULL");
+    HRM_GUARD(return collatz_run_noalloc(start, count, d_out_steps, cfg, res);)
+}

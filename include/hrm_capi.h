@@ -179,6 +179,25 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
 int hrm_bfs_run_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root,
                        uint32_t* d_levels, const hrm_run_config* cfg, hrm_run_result* res);
 
+/* ---- run without device allocation ------------------------------------------------------
+ * No counterpart in the original Harmonize (every original program instance allocates its
+ * buffers). For callers that cannot call cudaMalloc when they run a program: code recording
+ * into a CUDA stream capture that must not gain allocation nodes, plug-in hosts that only
+ * hand out buffers registered ahead of time, services that fix their memory use at start-up.
+ * Same result as hrm_collatz_run_device with AsyncProgram and variant 0, but the runtime's
+ * arena, queues and control block live in a scratch area compiled into the library (about
+ * 2.2 MiB, held on every GPU that loads the library until the process exits). The caller
+ * still passes the output buffer. Limits: cfg->arena may not exceed
+ * HRM_NOALLOC_MAX_ARENA_LINKS (0 means that maximum; larger is rejected with HRM_EINVAL), and
+ * a run whose promises in flight outgrow it stops with HRM_EDEVICE (ARENA_EXHAUSTED);
+ * program_type must be HRM_ASYNC and variant 0. The first call on each device looks up the
+ * scratch area's device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * All calls share the scratch area and each call re-initialises it; calls that overlap on
+ * the GPU race, so serialise them. res->device_ms is host wall time for this entry point. */
+#define HRM_NOALLOC_MAX_ARENA_LINKS 4096
+int hrm_collatz_run_device_noalloc(uint32_t start, uint32_t count, uint32_t* d_out_steps,
+                                   const hrm_run_config* cfg, hrm_run_result* res);
+
 /* ---- seeded synthetic inputs (host) ---------------------------------------------------- */
 
 /* R-MAT graph with 2^scale vertices and edge_factor * 2^scale edges, quadrant
