@@ -74,6 +74,11 @@ struct BfsSpec {
     static const size_t TEAMS_PER_CTA = TEAMS;
 
     template <typename PROGRAM>
+    HRM_DEV static void initialize(PROGRAM) {}
+    template <typename PROGRAM>
+    HRM_DEV static void finalize(PROGRAM) {}
+
+    template <typename PROGRAM>
     HRM_DEV static bool make_work(PROGRAM prog) {
         util::iter::Iter<unsigned int> it = prog.device.roots->leap(1u);
         unsigned int i;

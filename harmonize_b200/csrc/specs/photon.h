@@ -239,6 +239,11 @@ struct PhotonSpec {
     static const size_t TEAMS_PER_CTA = TEAMS;
 
     template <typename PROGRAM>
+    HRM_DEV static void initialize(PROGRAM) {}
+    template <typename PROGRAM>
+    HRM_DEV static void finalize(PROGRAM) {}
+
+    template <typename PROGRAM>
     HRM_DEV static bool make_work(PROGRAM prog) {
         // EventProgram: stop launching while the move buffer is loaded (load_fraction is NaN
         // under AsyncProgram, so the comparison is false there).

@@ -114,3 +114,87 @@ def philox(ctr, key):
 
 def log(x):
     return load().oracle_log(x)
+
+
+# ---------------------------------------------------------------------------------------
+# The reference CUDA build (oracle/_ref/libhrm_ref.so, see ref_build.py): the ORIGINAL
+# Harmonize runtime driving the same spec sources. Needs a GPU to run.
+# ---------------------------------------------------------------------------------------
+_ref = None
+
+
+def ref_load():
+    global _ref
+    if _ref is None:
+        from . import ref_build
+        path = ref_build.LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: build it with `python -m oracle.ref_build` where the "
+                                    f"reference tree is present")
+        L = ctypes.CDLL(path)
+        vp, u32, u64, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        fp, up = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32)
+        L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_collatz_run.restype = i32
+        L.ref_collatz_run.argtypes = [i32, u32, u32, vp, u32, u32, u32, u32, fp, up]
+        L.ref_photon_run_device.restype = i32
+        L.ref_photon_run_device.argtypes = [i32, vp, vp, vp, u32, u64, u32, u32, vp, u32, u32, u32, u32, fp, up]
+        L.ref_bfs_run_device.restype = i32
+        L.ref_bfs_run_device.argtypes = [i32, vp, vp, u32, u32, vp, u32, u32, u32, u32, fp, up]
+        _ref = L
+    return _ref
+
+
+def _ref_check(rc):
+    if rc != 0:
+        raise RuntimeError(f"reference runtime status {rc}: {ref_load().ref_last_error().decode(errors='replace')}")
+
+
+# Default launch shapes for the reference runtime: work groups of one warp, and the per-exec
+# cycle budget (AsyncProgram) or chunk (EventProgram) of its examples.
+REF_WG = 148 * 12
+REF_CYCLES = 0x1000000
+
+
+def ref_collatz(start, count, program="async", wg=REF_WG, n=None, arena=None, max_execs=20000):
+    pt = 0 if program == "async" else 1
+    n = n if n is not None else (REF_CYCLES if pt == 0 else 2)
+    arena = arena if arena is not None else (1 << 20)
+    out = np.zeros(count, dtype=np.uint32)
+    ms, ex = ctypes.c_float(), ctypes.c_uint32()
+    _ref_check(ref_load().ref_collatz_run(pt, start, count, out.ctypes.data, wg, n, arena, max_execs,
+                                          ctypes.byref(ms), ctypes.byref(ex)))
+    return out, {"ms": ms.value, "execs": ex.value}
+
+
+# The reference AsyncProgram raised an illegal memory access on the photon spec (record in
+# profiles/reference_asyncprogram_photon_fault.txt); it is suspected for every spec whose evals
+# make several async calls, so those specs run only on the reference EventProgram.
+REF_ASYNC_CLOSED = "reference AsyncProgram faulted (illegal memory access) on multi-call specs; not run again"
+
+
+def ref_photon_device(d_mu, d_ab, d_sp, n, seed, first, count, d_tally, program="event", wg=REF_WG, nn=None,
+                      arena=None, max_execs=200000):
+    """Pointers are device addresses (ints). Returns timing dict; tally left in d_tally."""
+    if program != "event":
+        raise RuntimeError(REF_ASYNC_CLOSED)
+    pt = 1
+    nn = nn if nn is not None else (REF_CYCLES if pt == 0 else 1)
+    arena = arena if arena is not None else ((1 << 20) if pt == 0 else (1 << 24))
+    ms, ex = ctypes.c_float(), ctypes.c_uint32()
+    _ref_check(ref_load().ref_photon_run_device(pt, d_mu, d_ab, d_sp, n, seed, first, count, d_tally, wg, nn, arena,
+                                                max_execs, ctypes.byref(ms), ctypes.byref(ex)))
+    return {"ms": ms.value, "execs": ex.value}
+
+
+def ref_bfs_device(d_rowptr, d_col, nv, root, d_levels, program="event", wg=REF_WG, nn=None, arena=None,
+                   max_execs=200000):
+    if program != "event":
+        raise RuntimeError(REF_ASYNC_CLOSED)
+    pt = 1
+    nn = nn if nn is not None else (REF_CYCLES if pt == 0 else 1)
+    arena = arena if arena is not None else ((1 << 20) if pt == 0 else (1 << 24))
+    ms, ex = ctypes.c_float(), ctypes.c_uint32()
+    _ref_check(ref_load().ref_bfs_run_device(pt, d_rowptr, d_col, nv, root, d_levels, wg, nn, arena, max_execs,
+                                             ctypes.byref(ms), ctypes.byref(ex)))
+    return {"ms": ms.value, "execs": ex.value}

@@ -1,0 +1,78 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every entry point declared in
+include/hrm_capi.h, and rejects bad arguments with status codes (no GPU needed)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hrm_capi.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hrm_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_life_cycle():
+    names = declared_functions()
+    for n in ["hrm_program_create", "hrm_program_init", "hrm_program_exec", "hrm_program_complete",
+              "hrm_program_clear_flags", "hrm_program_destroy", "hrm_last_error", "hrm_collatz_run",
+              "hrm_photon_run", "hrm_bfs_run", "hrm_collatz_run_device_noalloc"]:
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(hrm):
+    lib = ctypes.CDLL(hrm.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", hrm.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (hrm_\w+)", out))
+    assert set(declared_functions()) <= exported
+
+
+def test_header_compiles_as_c():
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", HEADER],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_bad_arguments_return_einval(hrm):
+    L = hrm.lib()
+    res = hrm.RunResult()
+    cfg = hrm.make_config("async")
+    assert L.hrm_photon_run(None, None, None, 16, 1, 0, 10, None, ctypes.byref(cfg), ctypes.byref(res)) == hrm.HRM_EINVAL
+    assert L.hrm_bfs_run(None, None, 4, 0, None, ctypes.byref(cfg), ctypes.byref(res)) == hrm.HRM_EINVAL
+    assert L.hrm_collatz_run(0, 10, None, ctypes.byref(cfg), ctypes.byref(res)) == hrm.HRM_EINVAL
+    h = ctypes.c_void_p()
+    state = ctypes.create_string_buffer(8)
+    rc = L.hrm_program_create(hrm.SPEC_COLLATZ, hrm.ASYNC, 0, state, 8, ctypes.byref(h))
+    assert rc == hrm.HRM_EINVAL and b"state size" in L.hrm_last_error()
+    rc = L.hrm_program_create(99, hrm.ASYNC, 0, state, 8, ctypes.byref(h))
+    assert rc == hrm.HRM_EINVAL
+    assert L.hrm_program_complete(None, None) == hrm.HRM_EINVAL
+
+
+def test_product_fails_loudly_without_its_library(monkeypatch, tmp_path):
+    import harmonize_b200 as h
+    monkeypatch.setattr(h, "_lib", None)
+    monkeypatch.setattr(h, "LIB_PATH", str(tmp_path / "missing.so"))
+    with pytest.raises(h.HarmonizeError):
+        h.collatz(0, 10)
+
+
+def test_inputs_are_deterministic(hrm):
+    rp1, c1 = hrm.rmat_csr(12, 8, seed=9)
+    rp2, c2 = hrm.rmat_csr(12, 8, seed=9)
+    assert np.array_equal(rp1, rp2) and np.array_equal(c1, c2)
+    assert rp1[-1] == len(c1) == 8 << 12 and np.all(np.diff(rp1.astype(np.int64)) >= 0)
+    m1 = hrm.photon_medium(8, 3)
+    m2 = hrm.photon_medium(8, 3)
+    assert all(np.array_equal(a, b) for a, b in zip(m1, m2))
+    mu, ab, sp = hrm.photon_medium(64, 1)
+    assert abs(np.log(mu).mean()) < 0.01 and abs(np.log(mu).std() - 0.5) < 0.01
+    assert ab.min() >= 0.02 and ab.max() <= 0.2 and abs(sp.mean() - 0.1) < 0.01

@@ -1,0 +1,111 @@
+"""CPU tests of the oracle: pinned to the reference runtime's own outputs (tests/golden, made by
+tests/golden/make_golden.py on a GPU) and to known answers; restatements against the host
+executors that run the very same spec sources as the GPU runtime."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_collatz_matches_reference_runtime_output():
+    ref = np.load(os.path.join(GOLDEN, "ref_collatz_0_4096.npy"))
+    assert np.array_equal(oracle.collatz_range(0, 4096), ref)
+
+
+def test_collatz_known_answers():
+    # Stopping times (OEIS A006577): 27 -> 111, 97 -> 118, 871 -> 178, 837799 -> 524 (the
+    # maximum below 10^6); 0 and 1 take no step, as in the reference checker.
+    steps = oracle.collatz_range(0, 1 << 20)
+    assert steps[0] == 0 and steps[1] == 0 and steps[2] == 1
+    assert steps[27] == 111 and steps[97] == 118 and steps[871] == 178
+    assert steps[837799] == 524 and steps.max() == 524
+    # evaluations of the Even/Odd program over n = 1..2^20: sum of (steps + 1)
+    total = int(steps[1:].astype(np.uint64).sum()) + (1 << 20) - 1 + 20 + 1
+    assert total == 139_348_407
+
+
+def test_collatz_executor_equals_restatement():
+    out, calls = oracle.exec_collatz(1000, 50000, threads=3)
+    ref = oracle.collatz_range(1000, 50000)
+    assert np.array_equal(out, ref)
+    assert int(calls.sum()) == int(ref.astype(np.uint64).sum()) + 50000
+
+
+def test_philox_known_answers():
+    # Known-answer vectors of Philox-4x32-10 (Salmon et al., SC'11; Random123 distribution).
+    assert [hex(x) for x in oracle.philox([0, 0, 0, 0], [0, 0])] == \
+        ["0x6627e8d5", "0xe169c58d", "0xbc57ac4c", "0x9b00dbd8"]
+    assert [hex(x) for x in oracle.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)] == \
+        ["0x408f276d", "0x41c83b0e", "0xa20bc7c6", "0x6d5451fd"]
+    assert [hex(x) for x in oracle.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344],
+                                          [0xA4093822, 0x299F31D0])] == \
+        ["0xd16cfe09", "0x94fdcceb", "0x5001e420", "0x24126ea1"]
+
+
+def test_log_accuracy():
+    rng = np.random.default_rng(3)
+    xs = np.concatenate([rng.random(4000).astype(np.float32) + np.float32(2 ** -24),
+                         np.float32(2.0) ** rng.integers(-24, 1, 200).astype(np.float32)])
+    for x in xs:
+        got = oracle.log(float(x))
+        exact = float(np.log(np.float64(x)))
+        ulp = float(np.spacing(np.float32(abs(exact)))) if exact != 0 else 1e-45
+        assert abs(got - exact) <= 4 * ulp + 1e-7 * abs(exact)
+
+
+def _medium16():
+    m = np.load(os.path.join(GOLDEN, "medium_n16_seed11.npz"))
+    return m["mu"], m["ab"], m["sp"]
+
+
+def test_photon_restatement_matches_reference_runtime_output():
+    mu, ab, sp = _medium16()
+    ref = np.load(os.path.join(GOLDEN, "ref_photon_n16_s99_500.npy"))
+    tally, _ = oracle.photon_walk(mu, ab, sp, 16, 99, 0, 500)
+    assert np.array_equal(tally, ref)
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+def test_photon_executor_equals_restatement(threads):
+    mu, ab, sp = _medium16()
+    a, ca = oracle.photon_walk(mu, ab, sp, 16, 0xC0FFEE, 77, 400)
+    b, cb = oracle.exec_photon(mu, ab, sp, 16, 0xC0FFEE, 77, 400, threads=threads)
+    assert np.array_equal(a, b)
+    assert np.array_equal(ca, cb)
+
+
+def test_photon_weight_conservation():
+    mu, ab, sp = _medium16()
+    n, count = 16, 1000
+    t, _ = oracle.photon_walk(mu, ab, sp, n, 5, 0, count)
+    v = n ** 3
+    S = oracle.PHOTON_SPREAD
+    total = int(t[:v].sum()) + int(t[v:v + S].sum()) + int(t[v + S:v + 2 * S].sum()) - int(t[v + 2 * S:].sum())
+    assert abs(total / 2 ** 32 - count) / count < 1e-5
+
+
+def test_bfs_restatement_matches_reference_runtime_output():
+    g = np.load(os.path.join(GOLDEN, "ref_bfs_rmat10.npz"))
+    assert np.array_equal(oracle.bfs(g["rowptr"], g["col"], 0), g["levels"])
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+def test_bfs_executor_equals_restatement(threads):
+    g = np.load(os.path.join(GOLDEN, "ref_bfs_rmat10.npz"))
+    lv, _ = oracle.exec_bfs(g["rowptr"], g["col"], 5, threads=threads)
+    assert np.array_equal(lv, oracle.bfs(g["rowptr"], g["col"], 5))
+
+
+def test_bfs_edge_cases():
+    # empty graph, isolated root, self loops and duplicate edges
+    rp = np.array([0, 0, 0], dtype=np.uint32)
+    assert list(oracle.bfs(rp, np.zeros(0, np.uint32), 1)) == [0xFFFFFFFF, 0]
+    rp = np.array([0, 3, 4, 4], dtype=np.uint32)
+    col = np.array([0, 1, 1, 2], dtype=np.uint32)
+    assert list(oracle.bfs(rp, col, 0)) == [0, 1, 2]
+    lv, _ = oracle.exec_bfs(rp, col, 0)
+    assert list(lv) == [0, 1, 2]
