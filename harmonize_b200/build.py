@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhrm.so")
-SOURCES = [os.path.join(HERE, "csrc", "hrm_capi.cu"), os.path.join(HERE, "csrc", "inputs.cpp")]
+SOURCES = [os.path.join(HERE, "csrc", "hrm_capi.cu"), os.path.join(HERE, "csrc", "hrm_batch.cu"),
+           os.path.join(HERE, "csrc", "inputs.cpp")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "-shared",

@@ -5,13 +5,16 @@
 // harmonize/python/templates.py:3-184).
 #include "../../include/harmonize.h"
 #include "../../include/hrm_capi.h"
+#include "capi_internal.h"
 #include "specs/bfs.h"
 #include "specs/collatz.h"
 #include "specs/photon.h"
 
 #include <chrono>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 namespace {
 
@@ -44,6 +47,11 @@ struct ProgramBase {
     virtual void clear_flags() = 0;
     virtual std::vector<unsigned long long> stats() = 0;
     virtual std::vector<unsigned int> overview() = 0;
+    virtual void set_state(const void* state, size_t size) = 0;
+    // Device scratch of the whole-run helpers (the start-value / source iterator), kept with
+    // the instance so that cached runs allocate nothing.
+    util::host::DevBuf<util::iter::AtomicIter<unsigned int>> iterator{(size_t)1};
+    std::mutex run_lock;  // one whole run at a time per cached instance
 };
 
 template <typename P>
@@ -63,6 +71,10 @@ struct ProgramImpl : ProgramBase {
     void clear_flags() override { inst.clear_flags(); }
     std::vector<unsigned long long> stats() override { return inst.read_stats(); }
     std::vector<unsigned int> overview() override { return inst.overview(); }
+    void set_state(const void* state, size_t size) override {
+        if (size != sizeof(typename P::DeviceState)) throw std::invalid_argument("device state size mismatch");
+        memcpy((void*)&inst.device_state, state, size);
+    }
 };
 
 static_assert(sizeof(hrm_collatz_state) == sizeof(hrm_specs::CollatzState), "collatz state layout");
@@ -196,6 +208,32 @@ struct DeviceArray {
     DeviceArray& operator=(const DeviceArray&) = delete;
 };
 
+// Program instances of the whole-run helpers, kept per (device, spec, type, variant,
+// arena) and re-initialised by every run, so that repeated runs allocate nothing.
+struct CacheKey {
+    int dev, spec, type, variant;
+    size_t arena;
+    bool operator<(const CacheKey& o) const {
+        return std::tie(dev, spec, type, variant, arena) < std::tie(o.dev, o.spec, o.type, o.variant, o.arena);
+    }
+};
+std::mutex g_cache_mutex;
+std::map<CacheKey, std::unique_ptr<ProgramBase>> g_cache;
+
+template <typename STATE>
+ProgramBase* cached_program(int spec, int type, int variant, size_t arena, const STATE& st) {
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    CacheKey key{dev, spec, type, variant, arena};
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    auto it = g_cache.find(key);
+    if (it == g_cache.end()) {
+        it = g_cache.emplace(key, std::unique_ptr<ProgramBase>(make_program(spec, type, arena, &st, sizeof(st),
+                                                                            variant))).first;
+    }
+    return it->second.get();
+}
+
 hrm_run_config config_or_default(const hrm_run_config* cfg) {
     hrm_run_config c;
     memset(&c, 0, sizeof(c));
@@ -207,18 +245,20 @@ int collatz_run(uint32_t start, uint32_t count, uint32_t* d_out, const hrm_run_c
     hrm_run_config cfg = config_or_default(cfg_in);
     if ((uint64_t)start + count > 0xFFFFFFFFull) return fail(HRM_EINVAL, "start + count exceeds 2^32");
     cudaStream_t s = (cudaStream_t)cfg.stream;
-    DeviceArray<util::iter::AtomicIter<unsigned int>> it(1);
-    util::iter::AtomicIter<unsigned int> host_it(start, start + count);
-    ck(cudaMemcpyAsync(it.ptr, &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     hrm_specs::CollatzState st;
     st.start = start;
     st.limit = start + count;
     st.output = d_out;
-    st.iterator = it.ptr;
+    st.iterator = nullptr;
     st.leap = 1;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_COLLATZ, cfg.program_type);
-    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_COLLATZ, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
-    return run_to_completion(p.get(), cfg, res);
+    ProgramBase* p = cached_program(HRM_SPEC_COLLATZ, cfg.program_type, cfg.variant, arena, st);
+    std::lock_guard<std::mutex> run(p->run_lock);
+    util::iter::AtomicIter<unsigned int> host_it(start, start + count);
+    ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    st.iterator = p->iterator.data();
+    p->set_state(&st, sizeof(st));
+    return run_to_completion(p, cfg, res);
 }
 
 // Photon walk with device-resident medium and tally (tally zeroed here).
@@ -230,15 +270,12 @@ int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32
     cudaStream_t s = (cudaStream_t)cfg.stream;
     const size_t slots = (size_t)n * n * n + 3u * hrm_specs::PHOTON_SPREAD;
     ck(cudaMemsetAsync(d_tally, 0, slots * sizeof(uint64_t), s), "tally clear");
-    DeviceArray<util::iter::AtomicIter<unsigned int>> it(1);
-    util::iter::AtomicIter<unsigned int> host_it(first, first + count);
-    ck(cudaMemcpyAsync(it.ptr, &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     hrm_specs::PhotonState st;
     st.mu_s = d_mu;
     st.absorb = d_ab;
     st.split = d_sp;
     st.tally = (unsigned long long*)d_tally;
-    st.source = it.ptr;
+    st.source = nullptr;
     st.n = n;
     st.seed_lo = (uint32_t)seed;
     st.seed_hi = (uint32_t)(seed >> 32);
@@ -247,8 +284,13 @@ int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32
     // splits grow a batch of photons several-fold before roulette thins it.
     st.load_limit = 0.015625f;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_PHOTON, cfg.program_type);
-    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_PHOTON, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
-    return run_to_completion(p.get(), cfg, res);
+    ProgramBase* p = cached_program(HRM_SPEC_PHOTON, cfg.program_type, cfg.variant, arena, st);
+    std::lock_guard<std::mutex> run(p->run_lock);
+    util::iter::AtomicIter<unsigned int> host_it(first, first + count);
+    ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    st.source = p->iterator.data();
+    p->set_state(&st, sizeof(st));
+    return run_to_completion(p, cfg, res);
 }
 
 // BFS over a device-resident CSR graph; levels initialised here.
@@ -258,19 +300,21 @@ int bfs_run(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32
     if (root >= nv) return fail(HRM_EINVAL, "root out of range");
     cudaStream_t s = (cudaStream_t)cfg.stream;
     ck(cudaMemsetAsync(d_levels, 0xFF, (size_t)nv * 4u, s), "levels init");
-    DeviceArray<util::iter::AtomicIter<unsigned int>> it(1);
-    util::iter::AtomicIter<unsigned int> host_it(0, 1);
-    ck(cudaMemcpyAsync(it.ptr, &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     hrm_specs::BfsState st;
     st.rowptr = d_rowptr;
     st.col = d_col;
     st.levels = d_levels;
-    st.roots = it.ptr;
+    st.roots = nullptr;
     st.root = root;
     st.nv = nv;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_BFS, cfg.program_type);
-    std::unique_ptr<ProgramBase> p(make_program(HRM_SPEC_BFS, cfg.program_type, arena, &st, sizeof(st), cfg.variant));
-    return run_to_completion(p.get(), cfg, res);
+    ProgramBase* p = cached_program(HRM_SPEC_BFS, cfg.program_type, cfg.variant, arena, st);
+    std::lock_guard<std::mutex> run(p->run_lock);
+    util::iter::AtomicIter<unsigned int> host_it(0, 1);
+    ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    st.roots = p->iterator.data();
+    p->set_state(&st, sizeof(st));
+    return run_to_completion(p, cfg, res);
 }
 
 }  // namespace
@@ -278,6 +322,8 @@ int bfs_run(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32
 struct hrm_program {
     ProgramBase* impl;
 };
+
+int hrm_capi::set_error(int code, const std::string& msg) { return fail(code, msg); }
 
 #define HRM_GUARD(...)                                           \
     try {                                                        \
@@ -302,6 +348,14 @@ int hrm_set_device(int device) {
 
 int hrm_device_sync(void) {
     HRM_GUARD(ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize"); return HRM_OK;)
+}
+
+int hrm_release_cache(void) {
+    HRM_GUARD({
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        g_cache.clear();
+        return HRM_OK;
+    })
 }
 
 int hrm_program_create(int spec, int program_type, size_t arena_or_io, const void* device_state, size_t state_size,

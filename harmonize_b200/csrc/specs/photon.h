@@ -227,6 +227,100 @@ HRM_HD HRM_FI Photon photon_source(const PhotonState& s, unsigned int id) {
     return p;
 }
 
+// The same walk without the async runtime: one thread follows a source photon and all of
+// its split descendants (explicit stack of `cap` entries), making the same tallies in the
+// same units. Used by the plain one-thread-per-photon baseline. Returns false if the stack
+// overflowed (the remaining descendants are dropped).
+template <unsigned int STACK = 48>
+HRM_HD HRM_FI bool photon_walk_thread(const PhotonState& s, unsigned int id, unsigned long long* calls) {
+    const unsigned int n = s.n;
+    const unsigned int S = PHOTON_SPREAD;
+    Photon stack[STACK];
+    unsigned int top = 0;
+    bool ok = true;
+    stack[top++] = photon_source(s, id);
+    unsigned long long k = 0;
+    while (top) {
+        Photon p = stack[--top];
+        while (true) {
+            k++;  // move
+            unsigned int ix = p.voxel % n, iy = (p.voxel / n) % n, iz = p.voxel / (n * n);
+            hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_MOVE);
+            float dist = hrm::fdiv(hrm::fsub(0.0f, hrm::log_exact(hrm::u01_open0(r.x))), s.mu_s[p.voxel]);
+            float tx = face_distance(p.x, p.dx, ix);
+            float ty = face_distance(p.y, p.dy, iy);
+            float tz = face_distance(p.z, p.dz, iz);
+            unsigned int axis = 0;
+            float tb = tx;
+            if (ty < tb) { tb = ty; axis = 1; }
+            if (tz < tb) { tb = tz; axis = 2; }
+            p.step += 1u;
+            if (dist < tb) {
+                p.x = hrm::fadd(p.x, hrm::fmul(dist, p.dx));
+                p.y = hrm::fadd(p.y, hrm::fmul(dist, p.dy));
+                p.z = hrm::fadd(p.z, hrm::fmul(dist, p.dz));
+                k++;  // collide
+                float dep = hrm::fmul(p.w, s.absorb[p.voxel]);
+                p.w = hrm::fsub(p.w, dep);
+                k++;
+                hrm::atomic_add_u64(&s.tally[p.voxel], to_fixed(dep));
+                if (p.w < WEIGHT_CUTOFF) {
+                    hrm::U32x4 rr = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_ROULETTE);
+                    unsigned int spread = p.id_lo & (S - 1u);
+                    k++;
+                    if (hrm::u01_open0(rr.x) <= ROULETTE_SURVIVAL) {
+                        float boosted = hrm::fmul(p.w, ROULETTE_BOOST);
+                        hrm::atomic_add_u64(&s.tally[n * n * n + 2u * S + spread], to_fixed(hrm::fsub(boosted, p.w)));
+                        p.w = boosted;
+                    } else {
+                        hrm::atomic_add_u64(&s.tally[n * n * n + S + spread], to_fixed(p.w));
+                        break;
+                    }
+                }
+                isotropic(s, p.id_lo, p.id_hi, p.step, p.dx, p.dy, p.dz);
+                p.step += 1u;
+                continue;
+            }
+            p.x = hrm::fadd(p.x, hrm::fmul(tb, p.dx));
+            p.y = hrm::fadd(p.y, hrm::fmul(tb, p.dy));
+            p.z = hrm::fadd(p.z, hrm::fmul(tb, p.dz));
+            bool out = false;
+            if (axis == 0) {
+                if (p.dx > 0.0f) { p.x = (float)(ix + 1u); out = (ix + 1u == n); ix += 1u; }
+                else { p.x = (float)ix; out = (ix == 0u); ix -= 1u; }
+            } else if (axis == 1) {
+                if (p.dy > 0.0f) { p.y = (float)(iy + 1u); out = (iy + 1u == n); iy += 1u; }
+                else { p.y = (float)iy; out = (iy == 0u); iy -= 1u; }
+            } else {
+                if (p.dz > 0.0f) { p.z = (float)(iz + 1u); out = (iz + 1u == n); iz += 1u; }
+                else { p.z = (float)iz; out = (iz == 0u); iz -= 1u; }
+            }
+            if (out) {
+                k++;
+                hrm::atomic_add_u64(&s.tally[n * n * n + (p.id_lo & (S - 1u))], to_fixed(p.w));
+                break;
+            }
+            p.voxel = ix + n * (iy + n * iz);
+            if (s.split[p.voxel]) {
+                p.w = hrm::fmul(p.w, 0.5f);
+                unsigned long long id64 = ((unsigned long long)p.id_hi << 32) | p.id_lo;
+                for (unsigned int c = 0; c < 2u; c++) {
+                    unsigned long long cid =
+                        hrm::mix64(id64 ^ (((unsigned long long)p.step << 1) | c) * 0x9E3779B97F4A7C15ull);
+                    Photon q = p;
+                    q.id_lo = (unsigned int)cid;
+                    q.id_hi = (unsigned int)(cid >> 32);
+                    if (top < STACK) stack[top++] = q;
+                    else ok = false;
+                }
+                break;
+            }
+        }
+    }
+    if (calls) *calls += k;
+    return ok;
+}
+
 template <size_t RING = 2, size_t TEAMS = 4>
 struct PhotonSpec {
     typedef OpUnion<PhotonMove, PhotonCollide, PhotonTally> OpSet;

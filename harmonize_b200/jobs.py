@@ -1,0 +1,141 @@
+"""Mixed job batches over the C ABI: the batched-instances and serving workloads.
+
+A job is one instance of a built-in spec (hrm_job in include/hrm_capi.h). make_mix builds
+the seeded synthetic mix of the batched configuration:
+  * Collatz ranges of length lognormal(median 2^12, sigma 1.5) clipped to [2^6, 2^20],
+    starting at a uniform value in [1, 2^21];
+  * photon-walk batches of 10^3..10^6 photons (log-uniform) on 32^3 grids, media drawn with
+    the same distributions (a pool of seeded media shared by the jobs);
+  * BFS from a random root on R-MAT graphs of 2^12..2^18 vertices, edge factor 16 (one seeded
+    graph per size, shared by the jobs).
+Device buffers are torch CUDA tensors kept alive by the Mix object.
+"""
+import ctypes
+
+import numpy as np
+
+from . import (HarmonizeError, RunResult, check, lib, make_config, photon_medium, rmat_csr)
+
+JOB_COLLATZ, JOB_PHOTON, JOB_BFS = 0, 1, 2
+KIND_NAMES = {JOB_COLLATZ: "collatz", JOB_PHOTON: "photon", JOB_BFS: "bfs"}
+PHOTON_SPREAD = 1024
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("first", ctypes.c_uint32), ("count", ctypes.c_uint32),
+                ("n", ctypes.c_uint32), ("seed", ctypes.c_uint64), ("a", ctypes.c_void_p),
+                ("b", ctypes.c_void_p), ("c", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
+def _bind():
+    L = lib()
+    if not getattr(L, "_jobs_bound", False):
+        L.hrm_batch_run.restype = ctypes.c_int
+        L.hrm_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p]
+        L.hrm_plain_run.restype = ctypes.c_int
+        L.hrm_plain_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                    ctypes.POINTER(ctypes.c_float)]
+        L._jobs_bound = True
+    return L
+
+
+class Mix:
+    """A list of jobs with their device inputs and two sets of device outputs (so that a
+    batched run and a plain run can be compared)."""
+
+    def __init__(self, specs, photon_grid=32, media=8, seed=1):
+        import torch
+        self.torch = torch
+        # list of dicts: kind, first, count / scale, medium / graph index
+        self.specs = [dict(s, medium=s["medium"] % media) if "medium" in s else dict(s) for s in specs]
+        self.grid = photon_grid
+        self.media = []
+        for m in range(media):
+            mu, ab, sp = photon_medium(photon_grid, seed * 1000 + m)
+            self.media.append(tuple(torch.from_numpy(x).cuda() for x in (mu, ab, sp)))
+        self.graphs = {}
+        for s in specs:
+            if s["kind"] == JOB_BFS and s["scale"] not in self.graphs:
+                rp, col = rmat_csr(s["scale"], 16, 0.57, 0.19, 0.19, seed * 100 + s["scale"])
+                self.graphs[s["scale"]] = (torch.from_numpy(rp.view(np.int32)).cuda(),
+                                           torch.from_numpy(col.view(np.int32)).cuda(), rp, col)
+        self.outputs = [self._alloc_outputs(), self._alloc_outputs()]
+
+    def _alloc_outputs(self):
+        torch = self.torch
+        outs = []
+        for s in self.specs:
+            if s["kind"] == JOB_COLLATZ:
+                outs.append(torch.empty(s["count"], dtype=torch.int32, device="cuda"))
+            elif s["kind"] == JOB_PHOTON:
+                outs.append(torch.empty(self.grid ** 3 + 3 * PHOTON_SPREAD, dtype=torch.int64, device="cuda"))
+            else:
+                outs.append(torch.empty(1 << s["scale"], dtype=torch.int32, device="cuda"))
+        return outs
+
+    def job_array(self, which=0, indices=None):
+        idx = range(len(self.specs)) if indices is None else indices
+        arr = (Job * len(idx))()
+        for k, i in enumerate(idx):
+            s = self.specs[i]
+            out = self.outputs[which][i].data_ptr()
+            if s["kind"] == JOB_COLLATZ:
+                arr[k] = Job(JOB_COLLATZ, s["first"], s["count"], 0, 0, None, None, None, out)
+            elif s["kind"] == JOB_PHOTON:
+                mu, ab, sp = self.media[s["medium"]]
+                arr[k] = Job(JOB_PHOTON, s["first"], s["count"], self.grid, s["seed"], mu.data_ptr(),
+                             ab.data_ptr(), sp.data_ptr(), out)
+            else:
+                d_rp, d_col, _, _ = self.graphs[s["scale"]]
+                arr[k] = Job(JOB_BFS, s["root"], 1, 1 << s["scale"], 0, d_rp.data_ptr(), d_col.data_ptr(), None,
+                             out)
+        return arr
+
+    def output(self, which, i):
+        t = self.outputs[which][i].cpu().numpy()
+        return t.view(np.uint64) if self.specs[i]["kind"] == JOB_PHOTON else t.view(np.uint32)
+
+    def total_work(self):
+        return {KIND_NAMES[k]: sum(1 for s in self.specs if s["kind"] == k) for k in KIND_NAMES}
+
+
+def make_mix_specs(njobs, seed=1, max_photons=1_000_000, max_scale=18, max_collatz=1 << 20):
+    """The seeded job mix (equal thirds of Collatz, photon and BFS jobs, interleaved)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for j in range(njobs):
+        kind = j % 3
+        if kind == JOB_COLLATZ:
+            length = int(np.clip(round(4096 * np.exp(1.5 * rng.standard_normal())), 64, max_collatz))
+            first = int(rng.integers(1, (1 << 21) + 1))
+            specs.append({"kind": JOB_COLLATZ, "first": first, "count": length})
+        elif kind == JOB_PHOTON:
+            count = int(round(10 ** rng.uniform(3.0, np.log10(max_photons))))
+            specs.append({"kind": JOB_PHOTON, "first": int(rng.integers(0, 1 << 30)), "count": count,
+                          "seed": int(rng.integers(1, 1 << 62)), "medium": int(rng.integers(0, 8))})
+        else:
+            scale = int(rng.integers(12, max_scale + 1))
+            specs.append({"kind": JOB_BFS, "scale": scale, "root": int(rng.integers(0, 1 << scale))})
+    return specs
+
+
+def batch_run(mix, which=0, indices=None, **cfg_kw):
+    """All (or the chosen) jobs in one persistent launch. Returns (done_ns array, result dict)."""
+    L = _bind()
+    arr = mix.job_array(which, indices)
+    done = np.zeros(len(arr), dtype=np.uint64)
+    cfg = make_config("async", **cfg_kw)
+    res = RunResult()
+    check(L.hrm_batch_run(ctypes.byref(arr), len(arr), ctypes.byref(cfg), ctypes.byref(res), done.ctypes.data))
+    return done, res.as_dict()
+
+
+def plain_run(mix, which=1, indices=None, streams=16):
+    """One plain-kernel launch per job. Returns (done_ns array, total ms)."""
+    L = _bind()
+    arr = mix.job_array(which, indices)
+    done = np.zeros(len(arr), dtype=np.uint64)
+    total = ctypes.c_float()
+    check(L.hrm_plain_run(ctypes.byref(arr), len(arr), streams, done.ctypes.data, ctypes.byref(total)))
+    return done, total.value

@@ -98,6 +98,10 @@ typedef struct hrm_run_result {
 const char* hrm_last_error(void);
 int hrm_set_device(int device);
 int hrm_device_sync(void);
+/* The whole-run helpers (hrm_*_run*) keep one program instance per device, spec, program
+ * type, variant and arena size, re-initialised by each run, so repeated runs allocate no
+ * device memory; concurrent runs on the same cached instance are serialised. This frees them. */
+int hrm_release_cache(void);
 
 /* ---- program life cycle (templates.py:3-184 counterparts) ------------------------------
  * hrm_program_create: spec + type + arena/io size + a copy of the spec's device state
@@ -178,6 +182,36 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
                 const hrm_run_config* cfg, hrm_run_result* res);
 int hrm_bfs_run_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root,
                        uint32_t* d_levels, const hrm_run_config* cfg, hrm_run_result* res);
+
+/* ---- many independent jobs --------------------------------------------------------------
+ * No counterpart in the original (one program instance per launch there). A job is one
+ * instance of a built-in spec; all pointers are device pointers owned by the caller. */
+#define HRM_JOB_COLLATZ 0
+#define HRM_JOB_PHOTON 1
+#define HRM_JOB_BFS 2
+typedef struct hrm_job {
+    uint32_t kind;      /* HRM_JOB_* */
+    uint32_t first;     /* collatz: first start value; photon: first photon id; bfs: root */
+    uint32_t count;     /* collatz: start values; photon: photons; bfs: unused */
+    uint32_t n;         /* photon: grid edge (even); bfs: vertex count */
+    uint64_t seed;      /* photon: Philox seed */
+    const void* a;      /* photon: float mu_s[n^3]; bfs: uint32 rowptr[n+1] */
+    const void* b;      /* photon: float absorb[n^3]; bfs: uint32 col[] */
+    const void* c;      /* photon: uint8 split[n^3] */
+    void* out;          /* collatz: uint32 steps[count]; photon: uint64 tally[n^3 + 3*1024];
+                           bfs: uint32 levels[n] */
+} hrm_job;
+
+/* All jobs in ONE persistent AsyncProgram launch (job-multiplexing spec; the launch sequence
+ * is a CUDA graph replayed per call). done_ns (host, njobs entries, may be NULL) receives each
+ * job's completion time in ns after the start of the device work. cfg->variant: R2/T4, R4/T4
+ * or R4/T2. Outputs equal those of one run per job, bit for bit. */
+int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg, hrm_run_result* res,
+                  uint64_t* done_ns);
+/* Baseline: one launch of a plain kernel per job (one thread per Collatz start value, one
+ * thread per source photon with its descendants, one CTA per BFS), jobs round-robin over
+ * nstreams streams. done_ns as above; *total_ms = time until the last job completed. */
+int hrm_plain_run(const hrm_job* jobs, uint32_t njobs, uint32_t nstreams, uint64_t* done_ns, float* total_ms);
 
 /* ---- run without device allocation ------------------------------------------------------
  * No counterpart in the original Harmonize (every original program instance allocates its
