@@ -36,15 +36,33 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compiles every translation unit to an object in parallel, then links libhrm.so."""
     if not force and not needs_build():
         return LIB
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        cmd = ["nvcc"] + ARCH + flags + list(extra) + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True), src))
+        objs.append(obj)
+    errors = []
+    for p, src in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            errors.append(f"{src}:\n{out}{err}")
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     tmp = LIB + ".tmp"
-    cmd = ["nvcc"] + ARCH + NVCC_FLAGS + list(extra) + ["-o", tmp] + SOURCES + ["-lgomp"]
-    if verbose:
-        print(" ".join(cmd))
+    cmd = ["nvcc"] + ARCH + ["-shared", "-Xcompiler", "-fopenmp", "-o", tmp] + objs + ["-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     os.replace(tmp, LIB)
     return LIB
 

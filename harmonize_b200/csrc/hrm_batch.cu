@@ -14,11 +14,15 @@
 #include "capi_internal.h"
 #include "specs/mix.h"
 
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstddef>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -105,6 +109,24 @@ __global__ void stamp_kernel(unsigned long long* t) {
     if (threadIdx.x == 0) *t = hrm_specs::global_ns();
 }
 
+// Clears the outputs of jobs [first, first+n) before they are published to a running kernel.
+__global__ void mix_prepare_range_kernel(JobRecord* jobs, unsigned int first, unsigned int n) {
+    for (unsigned int j = first + blockIdx.x; j < first + n; j += gridDim.x) {
+        JobRecord& r = jobs[j];
+        if (r.kind == hrm_specs::JOB_PHOTON) {
+            size_t slots = (size_t)r.s.p.n * r.s.p.n * r.s.p.n + 3u * hrm_specs::PHOTON_SPREAD;
+            for (size_t i = threadIdx.x; i < slots; i += blockDim.x) r.s.p.tally[i] = 0ull;
+        } else if (r.kind == hrm_specs::JOB_BFS) {
+            for (size_t i = threadIdx.x; i < r.s.b.nv; i += blockDim.x) r.s.b.levels[i] = 0xFFFFFFFFu;
+        }
+    }
+}
+
+// Asks a running exec to stop (the same request prog.halt_early() makes).
+__global__ void halt_kernel(hrm_rt::RuntimeControl* ctl) {
+    if (threadIdx.x == 0) atomicOr(&ctl->flags, hrm_rt::EARLY_HALT_FLAG);
+}
+
 // ---------------------------------------------------------------------------------------
 // Batch contexts: program instance + job table + counters, cached per (device, variant,
 // capacity, arena), with the launch sequence captured in a CUDA graph.
@@ -136,6 +158,7 @@ struct Batch : BatchBase {
         s.open = c + 2;
         s.completed = c + 3;
         s.closed = c + 4;
+        s.low = c + 5;
         s.done_host = nullptr;
         s.njobs = cap;
         return s;
@@ -321,9 +344,407 @@ __global__ void __launch_bounds__(1024) bfs_plain_block_kernel(const unsigned in
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Serving: a resident runtime that admits jobs while it runs.
+// ---------------------------------------------------------------------------------------
+struct ServerBase {
+    virtual ~ServerBase() {}
+    virtual unsigned int submit(const hrm_job* jobs, unsigned int n) = 0;  // returns first index
+    virtual unsigned int poll(uint64_t* done_ns, unsigned int max) = 0;    // returns completed count
+    virtual void close(unsigned int timeout_ms) = 0;
+    virtual size_t arena_bytes() const = 0;
+    virtual std::string describe_unfinished() = 0;
+    virtual volatile unsigned long long* done_flags() = 0;
+    virtual std::string error() = 0;
+};
+
+template <typename P>
+struct Server : ServerBase {
+    typename P::Instance inst;
+    util::host::DevBuf<JobRecord> jobs;
+    util::host::DevBuf<unsigned int> counters;  // admitted, cursor, open, completed, closed
+    unsigned long long* done_host = nullptr;    // mapped: %globaltimer of completion per job
+    JobRecord* staging = nullptr;               // pinned staging for job records
+    unsigned int* pinned_ctr = nullptr;         // pinned staging for counter writes
+    unsigned int capacity, submitted = 0;
+    size_t groups, cycles;
+    cudaStream_t exec_s = nullptr, submit_s = nullptr;
+    std::thread runner;
+    std::atomic<bool> host_open{true};
+    std::atomic<bool> stop{false};
+    std::mutex err_lock;
+    std::string err;
+    size_t arena_links;
+
+    Server(unsigned int cap, const hrm_run_config& cfg)
+        : inst((typename P::AdrType)(cfg.arena ? cfg.arena : ((size_t)1 << 21)), MixState{}),
+          jobs((size_t)cap),
+          counters((size_t)8),
+          capacity(cap),
+          groups(cfg.groups ? cfg.groups : (size_t)1 << 30),
+          cycles(cfg.cycles ? cfg.cycles : ((size_t)1 << 20)),
+          arena_links(cfg.arena ? cfg.arena : ((size_t)1 << 21)) {
+        ck(cudaHostAlloc((void**)&done_host, sizeof(unsigned long long) * cap, cudaHostAllocMapped), "done flags");
+        memset(done_host, 0, sizeof(unsigned long long) * cap);
+        unsigned long long* done_dev = nullptr;
+        ck(cudaHostGetDevicePointer((void**)&done_dev, done_host, 0), "done flags device alias");
+        ck(cudaHostAlloc((void**)&staging, sizeof(JobRecord) * 4096, cudaHostAllocDefault), "staging");
+        ck(cudaHostAlloc((void**)&pinned_ctr, sizeof(unsigned int) * 8, cudaHostAllocDefault), "staging");
+        ck(cudaStreamCreateWithFlags(&exec_s, cudaStreamNonBlocking), "stream");
+        ck(cudaStreamCreateWithFlags(&submit_s, cudaStreamNonBlocking), "stream");
+        MixState st = Batch<P>::state_for(jobs.data(), counters.data(), cap);
+        st.done_host = done_dev;
+        inst.device_state = st;
+        unsigned int ctr[8] = {0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
+        ck(cudaMemcpy(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice), "counters");
+        P::launch_init(inst, groups, exec_s);
+        ck(cudaStreamSynchronize(exec_s), "init");
+        runner = std::thread([this] { loop(); });
+    }
+
+    // Teardown is bounded: the session is closed, the running exec is asked to halt (teams
+    // leave within a few scheduling rounds, spilling their work), and the runner stops after
+    // that exec whether or not every job finished.
+    ~Server() {
+        host_open = false;
+        stop = true;
+        if (runner.joinable()) {
+            pinned_ctr[2] = 0;
+            cudaMemcpyAsync(counters.data() + 2, pinned_ctr + 2, 4, cudaMemcpyHostToDevice, submit_s);
+            halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
+            cudaStreamSynchronize(submit_s);
+            runner.join();
+        }
+        if (exec_s) cudaStreamDestroy(exec_s);
+        if (submit_s) cudaStreamDestroy(submit_s);
+        if (done_host) cudaFreeHost(done_host);
+        if (staging) cudaFreeHost(staging);
+        if (pinned_ctr) cudaFreeHost(pinned_ctr);
+    }
+
+    // Relaunches the persistent kernel until the session is closed and every job is done.
+    void loop() {
+        try {
+            while (true) {
+                P::launch_exec(inst, groups, cycles, exec_s);
+                ck(cudaStreamSynchronize(exec_s), "serving exec");
+                unsigned int f = inst.flags();
+                if (f & hrm_rt::ERROR_MASK) hrm_rt::throw_flags(f);
+                if (stop) break;
+                if (!host_open && (f & hrm_rt::COMPLETION_FLAG)) break;
+            }
+        } catch (std::exception& e) {
+            std::lock_guard<std::mutex> g(err_lock);
+            err = e.what();
+        }
+    }
+
+    unsigned int submit(const hrm_job* in, unsigned int n) override {
+        if (submitted + n > capacity) throw std::invalid_argument("server job table is full");
+        unsigned int first = submitted;
+        for (unsigned int done = 0; done < n;) {
+            unsigned int k = std::min(n - done, 4096u);
+            for (unsigned int i = 0; i < k; i++) {
+                if (job_sources(in[done + i]) == 0) throw std::invalid_argument("a served job needs work to do");
+                validate(in[done + i]);
+                staging[i] = make_record(in[done + i], jobs.data() + first + done + i);
+            }
+            ck(cudaMemcpyAsync(jobs.data() + first + done, staging, sizeof(JobRecord) * k, cudaMemcpyHostToDevice,
+                               submit_s), "job records");
+            ck(cudaStreamSynchronize(submit_s), "job records");
+            done += k;
+        }
+        mix_prepare_range_kernel<<<std::min(n, 1184u), 256, 0, submit_s>>>(jobs.data(), first, n);
+        ck(cudaGetLastError(), "output preparation");
+        pinned_ctr[0] = first + n;
+        // Published after the records (same stream): teams never see a job before its record.
+        ck(cudaMemcpyAsync(counters.data(), pinned_ctr, 4, cudaMemcpyHostToDevice, submit_s), "admit");
+        ck(cudaStreamSynchronize(submit_s), "admit");
+        submitted = first + n;
+        return first;
+    }
+
+    unsigned int poll(uint64_t* done_ns, unsigned int max) override {
+        unsigned int c = 0;
+        unsigned int m = std::min(max, submitted);
+        for (unsigned int j = 0; j < m; j++) {
+            unsigned long long t = ((volatile unsigned long long*)done_host)[j];
+            if (done_ns) done_ns[j] = t;
+            c += (t != 0ull);
+        }
+        return c;
+    }
+
+    void close(unsigned int timeout_ms) override {
+        host_open = false;
+        pinned_ctr[1] = 0;
+        ck(cudaMemcpyAsync(counters.data() + 2, pinned_ctr + 1, 4, cudaMemcpyHostToDevice, submit_s), "close");
+        ck(cudaStreamSynchronize(submit_s), "close");
+        auto t0 = std::chrono::steady_clock::now();
+        while (poll(nullptr, submitted) < submitted) {
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms)) {
+                throw std::runtime_error("serving session did not finish within the close timeout");
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+            std::string e = error();
+            if (!e.empty()) throw std::runtime_error(e);
+        }
+        if (runner.joinable()) runner.join();
+        std::string e = error();
+        if (!e.empty()) throw std::runtime_error(e);
+    }
+
+    // Device-side state of up to 8 unfinished jobs, for error messages.
+    std::string describe_unfinished() override {
+        std::vector<JobRecord> recs(submitted);
+        if (submitted == 0 || cudaMemcpy(recs.data(), jobs.data(), sizeof(JobRecord) * submitted,
+                                         cudaMemcpyDeviceToHost) != cudaSuccess)
+            return "";
+        unsigned int ctr[8] = {};
+        cudaMemcpy(ctr, counters.data(), sizeof(ctr), cudaMemcpyDeviceToHost);
+        std::string s = " [admitted " + std::to_string(ctr[0]) + " completed " + std::to_string(ctr[3]) + " closed " +
+                        std::to_string(ctr[4]) + " low " + std::to_string(ctr[5]) + " flags " +
+                        std::to_string(inst.flags()) + "]";
+        int shown = 0;
+        for (unsigned int j = 0; j < submitted && shown < 8; j++) {
+            const JobRecord& r = recs[j];
+            if (r.done) continue;
+            s += " job " + std::to_string(j) + ": kind " + std::to_string(r.kind) + " pending " +
+                 std::to_string(r.pending) + " source " + std::to_string(r.source.value) + "/" +
+                 std::to_string(r.source.limit) + " closed " + std::to_string(r.source_closed) + ";";
+            shown++;
+        }
+        return s;
+    }
+
+    size_t arena_bytes() const override { return arena_links * P::LINK_WORDS * 128u; }
+    volatile unsigned long long* done_flags() override { return done_host; }
+    std::string error() override {
+        std::lock_guard<std::mutex> g(err_lock);
+        return err;
+    }
+};
+
+ServerBase* make_server(unsigned int cap, const hrm_run_config& cfg) {
+    switch (cfg.variant) {
+        case HRM_VARIANT_R2_T4: return new Server<MixAsync<2, 4>>(cap, cfg);
+        case HRM_VARIANT_R4_T4: return new Server<MixAsync<4, 4>>(cap, cfg);
+        case HRM_VARIANT_R4_T2: return new Server<MixAsync<4, 2>>(cap, cfg);
+        default: throw std::invalid_argument("serving supports variants R2/T4, R4/T4 and R4/T2");
+    }
+}
+
+// Estimated arena bytes a job may occupy while in flight (admission control).
+size_t job_footprint(const hrm_job& j) {
+    size_t per = j.kind == HRM_JOB_PHOTON ? 48u : (j.kind == HRM_JOB_BFS ? 16u : 16u);
+    size_t items = j.kind == HRM_JOB_BFS ? ((size_t)j.n * 4u) : (size_t)j.count;
+    size_t b = items * per;
+    return b < ((size_t)64 << 20) ? b : ((size_t)64 << 20);
+}
+
 }  // namespace
 
+struct hrm_server {
+    ServerBase* impl;
+};
+
 extern "C" {
+
+int hrm_server_open(uint32_t capacity, const hrm_run_config* cfg_in, hrm_server** out) {
+    if (out == nullptr || capacity == 0) return hrm_capi::set_error(HRM_EINVAL, "bad server arguments");
+    try {
+        hrm_run_config cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        if (cfg_in) cfg = *cfg_in;
+        *out = new hrm_server{make_server(capacity, cfg)};
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_ECUDA, e.what());
+    }
+}
+
+int hrm_server_submit(hrm_server* srv, const hrm_job* jobs, uint32_t n, uint32_t* first_index) {
+    if (srv == nullptr || (jobs == nullptr && n)) return hrm_capi::set_error(HRM_EINVAL, "bad submit arguments");
+    try {
+        uint32_t f = srv->impl->submit(jobs, n);
+        if (first_index) *first_index = f;
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_ECUDA, e.what());
+    }
+}
+
+int hrm_server_poll(hrm_server* srv, uint64_t* done_ns, uint32_t max, uint32_t* completed) {
+    if (srv == nullptr) return hrm_capi::set_error(HRM_EINVAL, "server is NULL");
+    uint32_t c = srv->impl->poll(done_ns, max);
+    if (completed) *completed = c;
+    std::string e = srv->impl->error();
+    if (!e.empty()) return hrm_capi::set_error(HRM_EDEVICE, e);
+    return HRM_OK;
+}
+
+int hrm_server_close(hrm_server* srv, uint32_t timeout_ms) {
+    if (srv == nullptr) return hrm_capi::set_error(HRM_EINVAL, "server is NULL");
+    try {
+        srv->impl->close(timeout_ms);
+        return HRM_OK;
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_EDEVICE, e.what());
+    }
+}
+
+int hrm_server_destroy(hrm_server* srv) {
+    if (srv == nullptr) return HRM_OK;
+    delete srv->impl;
+    delete srv;
+    return HRM_OK;
+}
+
+// Replays an arrival schedule: arrival_ns[j] (non-decreasing, from the start of the call).
+// mode 0: the resident runtime (a server session, jobs admitted FIFO while their estimated
+// arena bytes fit half of the arena); mode 1: one plain launch per job at its arrival, on
+// nstreams streams. latency_ns[j] = host-observed completion - arrival.
+int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int mode, uint32_t nstreams,
+                     const hrm_run_config* cfg_in, uint64_t* latency_ns, float* makespan_ms) {
+    if ((jobs == nullptr || arrival_ns == nullptr || latency_ns == nullptr) && njobs)
+        return hrm_capi::set_error(HRM_EINVAL, "bad replay arguments");
+    using clk = std::chrono::steady_clock;
+    auto ns_since = [](clk::time_point t0) {
+        return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(clk::now() - t0).count();
+    };
+    try {
+        hrm_run_config cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        if (cfg_in) cfg = *cfg_in;
+        for (uint32_t j = 0; j < njobs; j++) validate(jobs[j]);
+        // Every replay ends: at the latest two minutes after the last arrival.
+        const uint64_t deadline_ns = (njobs ? arrival_ns[njobs - 1] : 0ull) + 120000000000ull;
+        if (mode == 0) {
+            std::unique_ptr<ServerBase> srv(make_server(njobs ? njobs : 1, cfg));
+            const size_t budget = srv->arena_bytes() / 2;
+            volatile unsigned long long* done = srv->done_flags();
+            std::vector<uint32_t> inflight;
+            size_t used = 0;
+            uint32_t next = 0, admitted = 0, finished = 0;
+            std::vector<hrm_job> batch;
+            auto t0 = clk::now();
+            while (finished < njobs) {
+                uint64_t now = ns_since(t0);
+                if (now > deadline_ns) {
+                    throw std::runtime_error("replay did not finish before its deadline; " + std::to_string(finished) +
+                                             " of " + std::to_string(njobs) + " done" + srv->describe_unfinished());
+                }
+                batch.clear();
+                while (admitted < njobs && arrival_ns[admitted] <= now) {
+                    size_t fp = job_footprint(jobs[admitted]);
+                    if (used + fp > budget && !inflight.empty()) break;
+                    used += fp;
+                    batch.push_back(jobs[admitted]);
+                    inflight.push_back(admitted);
+                    admitted++;
+                }
+                if (!batch.empty()) srv->submit(batch.data(), (unsigned int)batch.size());
+                for (size_t k = 0; k < inflight.size();) {
+                    uint32_t j = inflight[k];
+                    if (done[j] != 0ull) {
+                        latency_ns[j] = ns_since(t0) - arrival_ns[j];
+                        used -= job_footprint(jobs[j]);
+                        inflight[k] = inflight.back();
+                        inflight.pop_back();
+                        finished++;
+                    } else {
+                        k++;
+                    }
+                }
+                (void)next;
+                std::string e = srv->error();
+                if (!e.empty()) throw std::runtime_error(e);
+            }
+            if (makespan_ms) *makespan_ms = (float)(ns_since(t0) / 1e6);
+            srv->close(60000);
+        } else {
+            if (nstreams == 0) nstreams = 16;
+            std::vector<cudaStream_t> streams(nstreams);
+            for (auto& s : streams) ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+            std::vector<cudaEvent_t> ev(njobs);
+            for (auto& e : ev) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            size_t max_nv = 0;
+            for (uint32_t j = 0; j < njobs; j++)
+                if (jobs[j].kind == HRM_JOB_BFS && jobs[j].n > max_nv) max_nv = jobs[j].n;
+            unsigned int* d_ovf = nullptr;
+            unsigned int* d_fr = nullptr;
+            ck(cudaMalloc((void**)&d_ovf, 4), "overflow flag");
+            ck(cudaMemset(d_ovf, 0, 4), "overflow flag");
+            if (max_nv) ck(cudaMalloc((void**)&d_fr, max_nv * 2 * 4 * nstreams), "frontiers");
+            ck(cudaDeviceSynchronize(), "sync");
+            std::vector<uint32_t> inflight;
+            uint32_t launched = 0, finished = 0;
+            auto t0 = clk::now();
+            while (finished < njobs) {
+                uint64_t now = ns_since(t0);
+                if (now > deadline_ns) throw std::runtime_error("replay did not finish before its deadline");
+                while (launched < njobs && arrival_ns[launched] <= now) {
+                    const hrm_job& jb = jobs[launched];
+                    cudaStream_t s = streams[launched % nstreams];
+                    if (jb.kind == HRM_JOB_COLLATZ) {
+                        collatz_plain_kernel<<<(jb.count + 127) / 128, 128, 0, s>>>(jb.first, jb.count,
+                                                                                 (unsigned int*)jb.out);
+                    } else if (jb.kind == HRM_JOB_PHOTON) {
+                        size_t slots = (size_t)jb.n * jb.n * jb.n + 3u * hrm_specs::PHOTON_SPREAD;
+                        ck(cudaMemsetAsync(jb.out, 0, slots * 8u, s), "tally clear");
+                        hrm_specs::PhotonState st;
+                        memset(&st, 0, sizeof(st));
+                        st.mu_s = (const float*)jb.a;
+                        st.absorb = (const float*)jb.b;
+                        st.split = (const unsigned char*)jb.c;
+                        st.tally = (unsigned long long*)jb.out;
+                        st.n = jb.n;
+                        st.seed_lo = (unsigned int)jb.seed;
+                        st.seed_hi = (unsigned int)(jb.seed >> 32);
+                        photon_plain_kernel<<<(jb.count + 127) / 128, 128, 0, s>>>(st, jb.first, jb.count, d_ovf);
+                    } else {
+                        unsigned int* fr = d_fr + (size_t)(launched % nstreams) * max_nv * 2;
+                        bfs_plain_block_kernel<<<1, 1024, 0, s>>>((const unsigned int*)jb.a, (const unsigned int*)jb.b,
+                                                                  jb.n, jb.first, (unsigned int*)jb.out, fr,
+                                                                  fr + max_nv);
+                    }
+                    ck(cudaGetLastError(), "plain launch");
+                    ck(cudaEventRecord(ev[launched], s), "event");
+                    inflight.push_back(launched);
+                    launched++;
+                }
+                for (size_t k = 0; k < inflight.size();) {
+                    uint32_t j = inflight[k];
+                    cudaError_t q = cudaEventQuery(ev[j]);
+                    if (q == cudaSuccess) {
+                        latency_ns[j] = ns_since(t0) - arrival_ns[j];
+                        inflight[k] = inflight.back();
+                        inflight.pop_back();
+                        finished++;
+                    } else if (q == cudaErrorNotReady) {
+                        k++;
+                    } else {
+                        ck(q, "plain job");
+                    }
+                }
+            }
+            if (makespan_ms) *makespan_ms = (float)(ns_since(t0) / 1e6);
+            for (auto& s : streams) cudaStreamDestroy(s);
+            for (auto& e : ev) cudaEventDestroy(e);
+            cudaFree(d_ovf);
+            if (d_fr) cudaFree(d_fr);
+        }
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_EDEVICE, e.what());
+    }
+}
 
 int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg_in, hrm_run_result* res,
                   uint64_t* done_ns) {

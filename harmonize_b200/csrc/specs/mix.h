@@ -30,7 +30,10 @@ namespace hrm_specs {
 
 enum JobKind : unsigned int { JOB_COLLATZ = 0u, JOB_PHOTON = 1u, JOB_BFS = 2u };
 
-struct alignas(16) JobRecord {
+// One job per 128-byte-aligned record: records never share a cache line, so a team that
+// reads an admitted record cannot pull a not-yet-written neighbour into its SM's L1 (records
+// are written by the host while the serving kernel runs).
+struct alignas(128) JobRecord {
     unsigned int kind;
     int pending;                                 // promises alive + make_work tokens
     unsigned int done;                           // 1 once complete
@@ -54,6 +57,7 @@ struct MixState {
     unsigned int* completed;       // number of completed jobs
     unsigned int* closed;          // number of jobs whose source is exhausted (host closes
                                    // jobs with no source at all when it admits them)
+    unsigned int* low;             // every job below this index has an exhausted source
     unsigned long long* done_host; // host-mapped: t_done of each job (0 = not done), or null
     unsigned int njobs;            // capacity of the job table
 };
@@ -186,10 +190,11 @@ template <typename PROGRAM>
 HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int j) {
     JobRecord& r = st.jobs[j];
     int delta = 0;
-    if (r.kind == JOB_COLLATZ) {
+    const unsigned int kind = *(volatile unsigned int*)&r.kind;
+    if (kind == JOB_COLLATZ) {
         JobProgram<PROGRAM, CollatzState> jp{prog, r.s.c, j, &delta};
         CollatzSpec<>::template make_work<JobProgram<PROGRAM, CollatzState>>(jp);
-    } else if (r.kind == JOB_PHOTON) {
+    } else if (kind == JOB_PHOTON) {
         JobProgram<PROGRAM, PhotonState> jp{prog, r.s.p, j, &delta};
         PhotonSpec<>::template make_work<JobProgram<PROGRAM, PhotonState>>(jp);
     } else {
@@ -226,8 +231,16 @@ struct MixSpec {
         unsigned int admitted = *(volatile unsigned int*)st.admitted;
         unsigned int j = 0xFFFFFFFFu;
         if (lane == 0 && admitted > 0) {
+            // Advance the low watermark past jobs whose sources are exhausted, then probe
+            // round robin among [low, admitted).
+            unsigned int low = *(volatile unsigned int*)st.low;
+            while (low < admitted && *(volatile unsigned int*)&st.jobs[low].source_closed) {
+                low = atomicCAS(st.low, low, low + 1u) == low ? low + 1u : *(volatile unsigned int*)st.low;
+            }
+            unsigned int span = admitted > low ? admitted - low : 1u;
             for (unsigned int tries = 0; tries < 64u; tries++) {
-                unsigned int c = atomicAdd(st.cursor, 1u) % admitted;
+                unsigned int c = low + atomicAdd(st.cursor, 1u) % span;
+                if (c >= admitted) break;
                 JobRecord& r = st.jobs[c];
                 if (!r.source.done() && *(volatile unsigned int*)&r.done == 0u) {
                     j = c;

@@ -36,8 +36,72 @@ def _bind():
         L.hrm_plain_run.restype = ctypes.c_int
         L.hrm_plain_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                     ctypes.POINTER(ctypes.c_float)]
+        vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+        for name, args in {
+            "hrm_server_open": [u32, vp, ctypes.POINTER(vp)],
+            "hrm_server_submit": [vp, vp, u32, ctypes.POINTER(u32)],
+            "hrm_server_poll": [vp, vp, u32, ctypes.POINTER(u32)],
+            "hrm_server_close": [vp, u32],
+            "hrm_server_destroy": [vp],
+            "hrm_serve_replay": [vp, u32, vp, ctypes.c_int, u32, vp, vp, ctypes.POINTER(ctypes.c_float)],
+        }.items():
+            f = getattr(L, name)
+            f.restype = ctypes.c_int
+            f.argtypes = args
         L._jobs_bound = True
     return L
+
+
+class Server:
+    """A resident runtime session: submit jobs while it runs, poll completions, close."""
+
+    def __init__(self, capacity, **cfg_kw):
+        L = _bind()
+        self.cfg = make_config("async", **cfg_kw)
+        h = ctypes.c_void_p()
+        check(L.hrm_server_open(capacity, ctypes.byref(self.cfg), ctypes.byref(h)))
+        self.h = h
+        self.capacity = capacity
+
+    def submit(self, job_array):
+        first = ctypes.c_uint32()
+        check(_bind().hrm_server_submit(self.h, ctypes.byref(job_array), len(job_array), ctypes.byref(first)))
+        return first.value
+
+    def poll(self):
+        done = np.zeros(self.capacity, dtype=np.uint64)
+        c = ctypes.c_uint32()
+        check(_bind().hrm_server_poll(self.h, done.ctypes.data, self.capacity, ctypes.byref(c)))
+        return done, c.value
+
+    def close(self, timeout_ms=60000):
+        check(_bind().hrm_server_close(self.h, timeout_ms))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _bind().hrm_server_destroy(self.h)
+            self.h = None
+
+
+def serve_replay(mix, arrivals_ns, mode="resident", which=0, indices=None, streams=16, **cfg_kw):
+    """Replays arrival times against the resident runtime ("resident") or one plain launch per
+    job ("plain"). Returns (latency_ns array, makespan ms)."""
+    L = _bind()
+    arr = mix.job_array(which, indices)
+    arrivals = np.ascontiguousarray(arrivals_ns, dtype=np.uint64)
+    lat = np.zeros(len(arr), dtype=np.uint64)
+    span = ctypes.c_float()
+    cfg = make_config("async", **cfg_kw)
+    check(L.hrm_serve_replay(ctypes.byref(arr), len(arr), arrivals.ctypes.data, 0 if mode == "resident" else 1,
+                             streams, ctypes.byref(cfg), lat.ctypes.data, ctypes.byref(span)))
+    return lat, span.value
+
+
+def poisson_arrivals(n, rate_per_s, seed=11):
+    """Cumulative Poisson-process arrival times (ns) of n jobs at the given rate."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate_per_s, n)
+    return np.cumsum(gaps * 1e9).astype(np.uint64)
 
 
 class Mix:

@@ -676,11 +676,17 @@ class AsyncProgram {
                         if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
                         counted_idle = false;
                     }
+                    const unsigned int before = __reduce_add_sync(0xFFFFFFFFu, c);
                     bool more = hrm_rt::call_make_work<PROGRAM_SPEC>(*this);
                     can_make_work = __any_sync(0xFFFFFFFFu, more);
                     n_mw++;
                     clamp_counts();
-                    continue;
+                    const unsigned int after = __reduce_add_sync(0xFFFFFFFFu, (lane < FN) ? g.count[lane] : 0u);
+                    // New local work: plan again. Nothing local at all: keep asking. Otherwise
+                    // make_work added nothing, so run the partial batch held here instead of
+                    // waiting (a make_work that keeps returning true, e.g. a serving loop
+                    // polling for jobs, must not starve promises already in the stash).
+                    if (after != before || bc == 0) continue;
                 }
                 if (bc == 0) {
                     // Nothing local, nothing in the arena, nothing to make: idle.

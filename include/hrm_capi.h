@@ -213,6 +213,27 @@ int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg
  * nstreams streams. done_ns as above; *total_ms = time until the last job completed. */
 int hrm_plain_run(const hrm_job* jobs, uint32_t njobs, uint32_t nstreams, uint64_t* done_ns, float* total_ms);
 
+/* ---- serving: a resident runtime admitting jobs while it runs ---------------------------
+ * No counterpart in the original. hrm_server_open starts a persistent AsyncProgram over the
+ * job-multiplexing spec (a host thread relaunches its kernel while the session is open; queue
+ * state stays on the device between launches). hrm_server_submit appends jobs (each needs
+ * count >= 1) and publishes them to the running kernel; indices are in submission order.
+ * hrm_server_poll copies the completion stamps (%globaltimer ns, 0 = not done) of the first
+ * `max` jobs and counts completions. hrm_server_close stops admissions and waits for every
+ * submitted job. Capacity bounds the number of jobs per session. */
+typedef struct hrm_server hrm_server;
+int hrm_server_open(uint32_t capacity, const hrm_run_config* cfg, hrm_server** out);
+int hrm_server_submit(hrm_server* srv, const hrm_job* jobs, uint32_t n, uint32_t* first_index);
+int hrm_server_poll(hrm_server* srv, uint64_t* done_ns, uint32_t max, uint32_t* completed);
+int hrm_server_close(hrm_server* srv, uint32_t timeout_ms);
+int hrm_server_destroy(hrm_server* srv);
+/* Replays an arrival schedule (arrival_ns[j], non-decreasing, from the start of the call):
+ * mode 0 = the resident runtime (jobs admitted FIFO while their estimated arena bytes fit in
+ * half of the arena), mode 1 = one plain launch per job at its arrival on nstreams streams.
+ * latency_ns[j] = host-observed completion minus arrival; *makespan_ms = time to the last. */
+int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int mode, uint32_t nstreams,
+                     const hrm_run_config* cfg, uint64_t* latency_ns, float* makespan_ms);
+
 /* ---- run without device allocation ------------------------------------------------------
  * No counterpart in the original Harmonize (every original program instance allocates its
  * buffers). For callers that cannot call cudaMalloc when they run a program: code recording

@@ -1,0 +1,61 @@
+"""Serving: jobs admitted into the resident runtime while it runs. Each job's result must be the
+same alone and inside the mix (bit for bit), and the same as one plain launch per job."""
+import time
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def mix(hrm):
+    from harmonize_b200 import jobs
+    specs = jobs.make_mix_specs(36, seed=21, max_photons=2000, max_scale=12, max_collatz=1 << 13)
+    return jobs.Mix(specs, photon_grid=16, media=2, seed=21)
+
+
+@pytest.mark.gpu
+def test_server_results_same_alone_and_in_mix(hrm, mix):
+    from harmonize_b200 import jobs
+    n = len(mix.specs)
+    # alone: each job in its own session, one at a time (output set 1)
+    for i in range(n):
+        srv = jobs.Server(1, arena=1 << 16)
+        srv.submit(mix.job_array(1, [i]))
+        srv.close()
+        del srv
+    alone = [mix.output(1, i).copy() for i in range(n)]
+    # in the mix: all jobs submitted in small groups while the session runs (output set 0)
+    srv = jobs.Server(n, arena=1 << 18)
+    for g in range(0, n, 5):
+        srv.submit(mix.job_array(0, list(range(g, min(n, g + 5)))))
+        time.sleep(0.002)
+    srv.close()
+    done, completed = srv.poll()
+    assert completed == n and (done[:n] > 0).all()
+    for i in range(n):
+        assert np.array_equal(mix.output(0, i), alone[i]), (i, mix.specs[i])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["resident", "plain"])
+def test_replay_completes_every_job(hrm, mix, mode):
+    from harmonize_b200 import jobs
+    n = len(mix.specs)
+    arrivals = jobs.poisson_arrivals(n, rate_per_s=20000.0, seed=3)
+    lat, span = jobs.serve_replay(mix, arrivals, mode=mode, which=0, streams=4, arena=1 << 18)
+    assert (lat > 0).all() and span > 0
+    ref = [mix.output(0, i).copy() for i in range(n)]
+    jobs.plain_run(mix, which=1, streams=4)
+    for i in range(n):
+        assert np.array_equal(ref[i], mix.output(1, i))
+
+
+@pytest.mark.gpu
+def test_server_rejects_empty_jobs(hrm, mix):
+    from harmonize_b200 import jobs
+    arr = mix.job_array(0, [0])
+    arr[0].count = 0
+    srv = jobs.Server(2, arena=1 << 16)
+    with pytest.raises(hrm.HarmonizeError):
+        srv.submit(arr)
+    srv.close()
