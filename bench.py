@@ -40,7 +40,11 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="photon", choices=["photon", "bfs", "collatz"])
+    p.add_argument("--workload", default="photon", choices=["photon", "bfs", "collatz", "batched", "serving"])
+    p.add_argument("--jobs", type=int, default=4096, help="batched: number of job instances")
+    p.add_argument("--serve-jobs", type=int, default=512, help="serving: jobs per arrival-rate point")
+    p.add_argument("--rates", type=float, nargs="+", default=[0.1, 0.25, 0.5, 0.75, 0.9, 1.0, 1.25],
+                   help="serving: arrival rates as fractions of the batched throughput")
     p.add_argument("--program", default="async", choices=["async", "event"])
     p.add_argument("--photons", type=int, default=10_000_000)
     p.add_argument("--grid", type=int, default=128)
@@ -318,6 +322,81 @@ def run_collatz(args, hrm, rank, world, pg, torch):
                 bytes_per_call=BYTES_PER_CALL["collatz"], launches_per_step=3 if args.program == "async" else 2)
 
 
+def percentiles_ms(ns):
+    a = np.asarray(ns, dtype=np.float64) / 1e6
+    return {"p50": round(float(np.percentile(a, 50)), 3), "p99": round(float(np.percentile(a, 99)), 3),
+            "p99.9": round(float(np.percentile(a, 99.9)), 3), "max": round(float(a.max()), 3)}
+
+
+def run_batched(args):
+    """Batched uneven instances: the job mix in ONE persistent launch vs one plain launch per job."""
+    import torch
+    import harmonize_b200 as hrm
+    from harmonize_b200 import jobs
+    specs = jobs.make_mix_specs(args.jobs, seed=1)
+    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1)
+    variant = args.variant if args.variant >= 0 else 1
+    warm = list(range(min(48, args.jobs)))
+    jobs.batch_run(mix, 0, warm, variant=variant)
+    jobs.plain_run(mix, 1, warm)
+    with ClockSampler(0) as clk:
+        done_b, res = jobs.batch_run(mix, 0, variant=variant)
+        torch.cuda.synchronize()
+        done_p, plain_ms = jobs.plain_run(mix, 1, streams=16)
+    mism = [i for i in range(len(specs)) if not np.array_equal(mix.output(0, i), mix.output(1, i))]
+    if mism:
+        raise SystemExit(f"bench: {len(mism)} jobs differ between persistent and plain runs")
+    span_b = res["device_ms"]
+    calls = res["evals"]
+    line = {
+        "metric": "async calls/s", "value": round(calls / (span_b / 1e3), 1), "unit": "calls/s", "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": round(span_b, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+u64", "data": "synthetic",
+        "config": {"workload": f"batched_{args.jobs}_mixed_instances", "jobs": mix.total_work(),
+                   "variant": {"id": variant, "ring_links_teams_per_cta": list(hrm.VARIANTS[variant])},
+                   "persistent": "one launch (CUDA graph) of AsyncProgram<MixSpec>",
+                   "plain": "one launch per job, 16 streams"},
+        "jobs_per_s": {"persistent": round(args.jobs / (span_b / 1e3), 1),
+                       "plain": round(args.jobs / (plain_ms / 1e3), 1)},
+        "speedup_job_throughput": round(plain_ms / span_b, 3),
+        "completion_ms": {"persistent": percentiles_ms(done_b), "plain": percentiles_ms(done_p)},
+        "outputs": "identical per job (persistent vs plain)",
+        "full_batch_fraction": round(res["full_batches"] / max(1, res["batches"]), 4),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_serving(args):
+    """Serving: Poisson arrivals of the job mix, rate swept as fractions of the resident runtime's
+    batched throughput; resident runtime vs one plain launch per job at the same arrivals."""
+    import harmonize_b200 as hrm
+    from harmonize_b200 import jobs
+    n = args.serve_jobs
+    specs = jobs.make_mix_specs(n, seed=2)
+    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=2)
+    variant = args.variant if args.variant >= 0 else 1
+    done_b, res = jobs.batch_run(mix, 0, variant=variant)
+    sat = n / (res["device_ms"] / 1e3)
+    rows = []
+    for frac in args.rates:
+        rate = frac * sat
+        arr = jobs.poisson_arrivals(n, rate, seed=5)
+        lat_r, span_r = jobs.serve_replay(mix, arr, mode="resident", which=0, variant=variant)
+        lat_p, span_p = jobs.serve_replay(mix, arr, mode="plain", which=1, streams=16)
+        rows.append({"load": frac, "rate_jobs_per_s": round(rate, 1),
+                     "resident": dict(percentiles_ms(lat_r), jobs_per_s=round(n / (span_r / 1e3), 1)),
+                     "plain": dict(percentiles_ms(lat_p), jobs_per_s=round(n / (span_p / 1e3), 1))})
+        print(json.dumps(rows[-1]), flush=True)
+    mism = [i for i in range(n) if not np.array_equal(mix.output(0, i), mix.output(1, i))]
+    line = {"metric": "job latency p50/p99/p99.9 (ms) and job throughput", "workload": f"serving_{n}_jobs",
+            "saturation_jobs_per_s": round(sat, 1), "rates": rows,
+            "outputs": "identical per job" if not mism else f"{len(mism)} jobs differ"}
+    print(json.dumps(line), flush=True)
+    return line
+
+
 def pick_variant(args, hrm):
     """--variant, else the autotuner's choice for this workload and program type."""
     if args.variant >= 0:
@@ -335,6 +414,10 @@ def main():
     if args.impl == "reference":
         from oracle import reference_bench
         return reference_bench.main(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "serving":
+        return run_serving(args)
     import torch
     import harmonize_b200 as hrm
     rank, world, local, pg = dist_setup(args)

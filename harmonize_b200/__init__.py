@@ -92,6 +92,7 @@ def lib():
                                       ctypes.POINTER(RunResult)],
             "hrm_bfs_run": [vp, vp, u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
             "hrm_bfs_run_device": [vp, vp, u32, u32, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
+            "hrm_barrier_demo_run": [u32, u32, u32, vp, vp, ctypes.POINTER(RunConfig), ctypes.POINTER(RunResult)],
             "hrm_rmat_csr": [u32, u32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, vp, vp],
             "hrm_photon_medium": [u32, ctypes.c_uint64, vp, vp, vp],
         }
@@ -244,3 +245,17 @@ class Program:
             self.close()
         except Exception:
             pass
+
+
+def barrier_demo(dep_count, non_dep_count, barrier_count, program="async", **kw):
+    """The remapping-barrier workload (examples/cpp/barrier_demo/demo.cpp:20-86 of Harmonize).
+
+    Returns (counter uint32[4], released uint32[barrier_count], run-result dict); counter is
+    (Steps run, non-dependent Steps, final Steps, violations)."""
+    counter = np.zeros(4, dtype=np.uint32)
+    released = np.zeros(max(barrier_count, 1), dtype=np.uint32)
+    cfg = make_config(program, **kw)
+    res = RunResult()
+    check(lib().hrm_barrier_demo_run(dep_count, non_dep_count, barrier_count, counter.ctypes.data,
+                                     released.ctypes.data, ctypes.byref(cfg), ctypes.byref(res)))
+    return counter, released, res.as_dict()

@@ -159,6 +159,8 @@ struct Batch : BatchBase {
         s.completed = c + 3;
         s.closed = c + 4;
         s.low = c + 5;
+        s.started = c + 6;
+        s.max_active = 256;
         s.done_host = nullptr;
         s.njobs = cap;
         return s;
@@ -629,7 +631,7 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
             volatile unsigned long long* done = srv->done_flags();
             std::vector<uint32_t> inflight;
             size_t used = 0;
-            uint32_t next = 0, admitted = 0, finished = 0;
+            uint32_t admitted = 0, finished = 0;
             std::vector<hrm_job> batch;
             auto t0 = clk::now();
             while (finished < njobs) {
@@ -660,7 +662,6 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
                         k++;
                     }
                 }
-                (void)next;
                 std::string e = srv->error();
                 if (!e.empty()) throw std::runtime_error(e);
             }
@@ -755,7 +756,9 @@ int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg
         if (cfg_in) cfg = *cfg_in;
         if (cfg.program_type != HRM_ASYNC) throw std::invalid_argument("batched runs use AsyncProgram");
         for (uint32_t j = 0; j < njobs; j++) validate(jobs[j]);
-        size_t arena = cfg.arena ? cfg.arena : ((size_t)1 << 21);
+        // Default arena: 2^23 links (about 12 GB for the mixed spec). Thousands of BFS jobs
+        // fan out millions of relaxations at once and none of that can be throttled.
+        size_t arena = cfg.arena ? cfg.arena : ((size_t)1 << 23);
         BatchBase* b = batch_for(cfg.variant, njobs ? njobs : 1, arena);
         JobRecord* d_table = b->table();  // records point into the cached context's job table
         std::vector<JobRecord> recs(njobs);

@@ -6,6 +6,7 @@
 #include "../../include/harmonize.h"
 #include "../../include/hrm_capi.h"
 #include "capi_internal.h"
+#include "specs/barrier_demo.h"
 #include "specs/bfs.h"
 #include "specs/collatz.h"
 #include "specs/photon.h"
@@ -80,6 +81,7 @@ struct ProgramImpl : ProgramBase {
 static_assert(sizeof(hrm_collatz_state) == sizeof(hrm_specs::CollatzState), "collatz state layout");
 static_assert(sizeof(hrm_photon_state) == sizeof(hrm_specs::PhotonState), "photon state layout");
 static_assert(sizeof(hrm_bfs_state) == sizeof(hrm_specs::BfsState), "bfs state layout");
+static_assert(sizeof(hrm_barrier_demo_state) == sizeof(hrm_specs::BarrierDemoState), "barrier demo state layout");
 
 template <typename STATE>
 STATE state_from(const void* p, size_t n) {
@@ -132,6 +134,18 @@ ProgramBase* make_program(int spec, int type, size_t arena, const void* state, s
         case HRM_SPEC_BFS: {
             auto s = state_from<hrm_specs::BfsState>(state, state_size);
             p = make_variant<hrm_specs::BfsSpec>(type, variant, arena, s);
+            break;
+        }
+        case HRM_SPEC_BARRIER_DEMO: {
+            // Barriers hold promises in the AsyncProgram arena: no EventProgram form.
+            if (type != HRM_ASYNC) throw std::invalid_argument("the barrier demo runs on AsyncProgram only");
+            auto s = state_from<hrm_specs::BarrierDemoState>(state, state_size);
+            if (s.barrier_count == 0) throw std::invalid_argument("barrier_count must be >= 1");
+            switch (variant) {
+                case HRM_VARIANT_R2_T4: p = new ProgramImpl<AsyncProgram<hrm_specs::BarrierDemoSpec<2, 4>>>(arena, s); break;
+                case HRM_VARIANT_R4_T4: p = new ProgramImpl<AsyncProgram<hrm_specs::BarrierDemoSpec<4, 4>>>(arena, s); break;
+                default: throw std::invalid_argument("the barrier demo is built for variants R2/T4 and R4/T4");
+            }
             break;
         }
         default:
@@ -315,6 +329,52 @@ int bfs_run(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32
     st.roots = p->iterator.data();
     p->set_state(&st, sizeof(st));
     return run_to_completion(p, cfg, res);
+}
+
+// Remapping-barrier workload; counters and barriers are set up here, results copied out.
+int barrier_demo_run(uint32_t dep, uint32_t ndep, uint32_t bar, uint32_t* counter, uint32_t* released,
+                     const hrm_run_config* cfg_in, hrm_run_result* res) {
+    hrm_run_config cfg = config_or_default(cfg_in);
+    if (bar == 0) return fail(HRM_EINVAL, "barrier_count must be >= 1");
+    if ((uint64_t)dep + ndep >= hrm_specs::BARRIER_FINAL) return fail(HRM_EINVAL, "dep + ndep too large");
+    if (cfg.program_type != HRM_ASYNC) return fail(HRM_EINVAL, "the barrier demo runs on AsyncProgram only");
+    cudaStream_t s = (cudaStream_t)cfg.stream;
+    using Barrier = RemappingBarrier<hrm_specs::BarrierOps>;
+    using Unit = UnitBarrier<hrm_specs::BarrierOps>;
+    // Barrier b waits for the dependent ids congruent to b (demo.cpp:163-170).
+    std::vector<Barrier> bars(bar);
+    for (uint32_t b = 0; b < bar; b++) bars[b] = Barrier::blank(dep / bar + ((dep % bar) > b ? 1u : 0u));
+    Unit unit(PromiseEnum<hrm_specs::BarrierOps>(Promise<hrm_specs::BarrierStep>(hrm_specs::BARRIER_FINAL)), ndep);
+    DeviceArray<Barrier> dbars(bar);
+    DeviceArray<Unit> dunit(1);
+    DeviceArray<uint32_t> dcount(4), drel(bar);
+    ck(cudaMemcpyAsync(dbars.ptr, bars.data(), sizeof(Barrier) * bar, cudaMemcpyHostToDevice, s), "barrier upload");
+    ck(cudaMemcpyAsync(dunit.ptr, &unit, sizeof(Unit), cudaMemcpyHostToDevice, s), "barrier upload");
+    ck(cudaMemsetAsync(dcount.ptr, 0, 16, s), "counter clear");
+    ck(cudaMemsetAsync(drel.ptr, 0, (size_t)bar * 4u, s), "counter clear");
+    hrm_specs::BarrierDemoState st;
+    st.dep_count = dep;
+    st.non_dep_count = ndep;
+    st.barrier_count = bar;
+    st.pad = 0;
+    st.source = nullptr;
+    st.counter = dcount.ptr;
+    st.released = drel.ptr;
+    st.barriers = dbars.ptr;
+    st.unit = dunit.ptr;
+    size_t arena = cfg.arena ? cfg.arena : ((size_t)1 << 18);
+    ProgramBase* p = cached_program(HRM_SPEC_BARRIER_DEMO, HRM_ASYNC, cfg.variant, arena, st);
+    std::lock_guard<std::mutex> run(p->run_lock);
+    util::iter::AtomicIter<unsigned int> host_it(0, dep + ndep);
+    ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
+    st.source = p->iterator.data();
+    p->set_state(&st, sizeof(st));
+    int rc = run_to_completion(p, cfg, res);
+    if (rc != HRM_OK) return rc;
+    ck(cudaMemcpyAsync(counter, dcount.ptr, 16, cudaMemcpyDeviceToHost, s), "counter download");
+    ck(cudaMemcpyAsync(released, drel.ptr, (size_t)bar * 4u, cudaMemcpyDeviceToHost, s), "counter download");
+    ck(cudaStreamSynchronize(s), "counter download");
+    return HRM_OK;
 }
 
 }  // namespace
@@ -526,6 +586,12 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
         ck(cudaStreamSynchronize(s), "levels download");
         return HRM_OK;
     })
+}
+
+int hrm_barrier_demo_run(uint32_t dep_count, uint32_t non_dep_count, uint32_t barrier_count, uint32_t* counter,
+                         uint32_t* released, const hrm_run_config* cfg, hrm_run_result* res) {
+    if (!counter || !released) return fail(HRM_EINVAL, "NULL buffer");
+    HRM_GUARD(return barrier_demo_run(dep_count, non_dep_count, barrier_count, counter, released, cfg, res);)
 }
 
 }  // extern "C"

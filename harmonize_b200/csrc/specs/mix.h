@@ -58,6 +58,8 @@ struct MixState {
     unsigned int* closed;          // number of jobs whose source is exhausted (host closes
                                    // jobs with no source at all when it admits them)
     unsigned int* low;             // every job below this index has an exhausted source
+    unsigned int* started;         // jobs that have received their first make_work
+    unsigned int max_active;       // a job starts only while started - completed < max_active
     unsigned long long* done_host; // host-mapped: t_done of each job (0 = not done), or null
     unsigned int njobs;            // capacity of the job table
 };
@@ -128,20 +130,110 @@ HRM_DEV HRM_FI void job_complete(const MixState& st, unsigned int j) {
 #endif
 }
 
-// Adds `delta` to job j's pending count, one atomic per group of lanes with the same job;
-// completes the job when the count returns to zero with its source exhausted.
-HRM_DEV HRM_FI void job_settle(const MixState& st, unsigned int j, int delta) {
+// Per-team bookkeeping (the mix spec's GroupState, in shared memory).
+//
+// Each evaluation records, in its lane's slot, its job and its change of that job's
+// pending count (promises created minus the one consumed). After the batch the whole team
+// settles the slots together (after_batch): lanes are grouped by job, net increments are
+// published at once and net decrements are deferred in a small table keyed by job.
+//
+// Why deferring decrements is safe: a job is declared complete when its published count
+// reaches zero. Increments are published before the new promises can leave the team (they
+// sit in the team's private rings until a spill, and a spill publishes with a fence), so
+// the published count never drops below the number of promises alive; holding a decrement
+// back only keeps it higher. Decrements are published, with one fence per flush instead of
+// one per batch, when an entry is evicted, every FLUSH_EVERY batches, and whenever the
+// team runs out of work (make_work, on_idle, finalize), so no completion is held back
+// while the team sleeps.
+struct MixTeam {
+    static const unsigned int SLOTS = 8;
+    static const unsigned int FLUSH_EVERY = 16;
+    static const unsigned int EMPTY = 0xFFFFFFFFu;
+    unsigned int lane_job[32];  // job of the lane's evaluation in this batch, or EMPTY
+    int lane_delta[32];
+    unsigned int job[SLOTS];
+    int delta[SLOTS];
+    unsigned int settles;
+    unsigned int used;  // bit s set while job[s] holds an entry
+};
+
+// One lane: publishes a decrement of job j, completing the job at zero with its source
+// exhausted. The fence orders this team's writes of the job's results before the count.
+HRM_DEV HRM_FI void job_publish(const MixState& st, unsigned int j, int d) {
 #if defined(__CUDA_ARCH__)
-    unsigned int mask = __activemask();
-    unsigned int grp = __match_any_sync(mask, j);
-    int sum = (int)__reduce_add_sync(grp, (unsigned int)delta);
+    __threadfence();
+    int old = atomicAdd(&st.jobs[j].pending, d);
+    if (old + d == 0 && st.jobs[j].source.done()) job_complete(st, j);
+#endif
+}
+
+// One lane: publishes every deferred decrement of the team.
+HRM_DEV HRM_FI void team_flush(const MixState& st, MixTeam& t) {
+#if defined(__CUDA_ARCH__)
+    unsigned int used = t.used;
+    if (used != 0u) {
+        __threadfence();
+        while (used) {
+            unsigned int s = __ffs(used) - 1;
+            used &= used - 1;
+            int d = t.delta[s];
+            int old = atomicAdd(&st.jobs[t.job[s]].pending, d);
+            if (old + d == 0 && st.jobs[t.job[s]].source.done()) job_complete(st, t.job[s]);
+            t.job[s] = MixTeam::EMPTY;
+        }
+        t.used = 0u;
+    }
+    t.settles = 0u;
+#endif
+}
+
+// One lane: records a decrement of job j in the team table.
+HRM_DEV HRM_FI void team_defer(const MixState& st, MixTeam& t, unsigned int j, int d) {
+    const unsigned int s = j & (MixTeam::SLOTS - 1u);
+    const unsigned int bit = 1u << s;
+    if ((t.used & bit) != 0u && t.job[s] == j) {
+        t.delta[s] += d;
+        return;
+    }
+    if ((t.used & bit) != 0u) job_publish(st, t.job[s], t.delta[s]);  // evict the other job
+    t.job[s] = j;
+    t.delta[s] = d;
+    t.used |= bit;
+}
+
+// Whole team, converged: settles the lane slots of the batch just evaluated.
+HRM_DEV HRM_FI void team_settle(const MixState& st, MixTeam& t) {
+#if defined(__CUDA_ARCH__)
     unsigned int lane;
     asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
-    if (lane == (unsigned int)(__ffs(grp) - 1) && sum != 0) {
-        __threadfence();
-        int old = atomicAdd(&st.jobs[j].pending, sum);
-        if (old + sum == 0 && st.jobs[j].source.done()) job_complete(st, j);
+    const unsigned int j = t.lane_job[lane];
+    const int delta = t.lane_delta[lane];
+    t.lane_job[lane] = MixTeam::EMPTY;
+    const unsigned int grp = __match_any_sync(0xFFFFFFFFu, j);
+    const int sum = (int)__reduce_add_sync(grp, (unsigned int)delta);
+    const bool leader = j != MixTeam::EMPTY && lane == (unsigned int)(__ffs(grp) - 1);
+    if (leader && sum > 0) atomicAdd(&st.jobs[j].pending, sum);  // a rising count completes nothing
+    unsigned int defer = __ballot_sync(0xFFFFFFFFu, leader && sum < 0);
+    // One lane at a time updates the table (it belongs to this team alone).
+    while (defer) {
+        const unsigned int src = __ffs(defer) - 1;
+        defer &= defer - 1;
+        if (lane == src) team_defer(st, t, j, sum);
+        __syncwarp();
     }
+    if (lane == 0 && ++t.settles >= MixTeam::FLUSH_EVERY) team_flush(st, t);
+    __syncwarp();
+#endif
+}
+
+// Whole team: publishes every deferred decrement.
+HRM_DEV HRM_FI void team_flush_all(const MixState& st, MixTeam& t) {
+#if defined(__CUDA_ARCH__)
+    __syncwarp();
+    unsigned int lane;
+    asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
+    if (lane == 0) team_flush(st, t);
+    __syncwarp();
 #endif
 }
 
@@ -181,7 +273,11 @@ struct Job {
         int delta = -1;
         JobProgram<PROGRAM, S> jp{prog, inner_state, job, &delta};
         F::template eval<JobProgram<PROGRAM, S>>(jp, a...);
-        job_settle(st, job, delta);
+        // Settled by the whole team after the batch (MixSpec::after_batch).
+        MixTeam& t = prog.group;
+        const unsigned int lane = util::lane_id();
+        t.lane_job[lane] = job;
+        t.lane_delta[lane] = delta;
     }
 };
 
@@ -204,21 +300,51 @@ HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int 
     return delta;
 }
 
+// RING: ring links of the two photon functions whose promises carry a whole photon (move,
+// collide: 12 words each); every other function (5 words or fewer) gets 2 links, which
+// keeps a team's stash small enough for 12-16 resident teams per SM.
 template <size_t RING = 4, size_t TEAMS = 4>
 struct MixSpec {
     typedef OpUnion<Job<CollatzEven>, Job<CollatzOdd>, Job<PhotonMove>, Job<PhotonCollide>, Job<PhotonTally>,
                     Job<BfsRelax>, Job<BfsExpand>>
         OpSet;
     typedef MixState DeviceState;
+    typedef MixTeam GroupState;
 
     static const size_t STASH_SIZE = 16;
-    static const size_t RING_LINKS = RING;
+    static const size_t RING_LINKS = 2;
     static const size_t TEAMS_PER_CTA = TEAMS;
+    template <typename Op>
+    struct RING_LINKS_OF {
+        static const size_t value =
+            (std::is_same<Op, Job<PhotonMove>>::value || std::is_same<Op, Job<PhotonCollide>>::value) ? RING : 2;
+    };
 
     template <typename PROGRAM>
-    HRM_DEV static void initialize(PROGRAM) {}
+    HRM_DEV static void initialize(PROGRAM prog) {
+        MixTeam& t = prog.group;
+        const unsigned int lane = util::lane_id();
+        t.lane_job[lane] = MixTeam::EMPTY;
+        t.lane_delta[lane] = 0;
+        if (lane < MixTeam::SLOTS) t.job[lane] = MixTeam::EMPTY;
+        if (lane == 0) {
+            t.settles = 0;
+            t.used = 0;
+        }
+        __syncwarp();
+    }
     template <typename PROGRAM>
-    HRM_DEV static void finalize(PROGRAM) {}
+    HRM_DEV static void finalize(PROGRAM prog) {
+        team_flush_all(prog.device, prog.group);
+    }
+    template <typename PROGRAM>
+    HRM_DEV static void on_idle(PROGRAM prog) {
+        team_flush_all(prog.device, prog.group);
+    }
+    template <typename PROGRAM>
+    HRM_DEV static void after_batch(PROGRAM prog) {
+        team_settle(prog.device, prog.group);
+    }
 
     // Called by a whole team: picks one job that still has sources (round robin over the
     // admitted jobs), takes a token on it, makes its share of work, settles the count.
@@ -226,6 +352,7 @@ struct MixSpec {
     HRM_DEV static bool make_work(PROGRAM prog) {
 #if defined(__CUDA_ARCH__)
         const MixState& st = prog.device;
+        team_flush_all(st, prog.group);
         unsigned int lane;
         asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
         unsigned int admitted = *(volatile unsigned int*)st.admitted;
@@ -243,9 +370,16 @@ struct MixSpec {
                 if (c >= admitted) break;
                 JobRecord& r = st.jobs[c];
                 if (!r.source.done() && *(volatile unsigned int*)&r.done == 0u) {
+                    if (*(volatile unsigned long long*)&r.t_admit == 0ull) {
+                        // Not started yet: start it only while fewer than max_active jobs
+                        // are in progress (bounds the promises in flight).
+                        unsigned int active = *(volatile unsigned int*)st.started -
+                                              *(volatile unsigned int*)st.completed;
+                        if (active >= st.max_active) continue;
+                        if (atomicCAS(&r.t_admit, 0ull, global_ns()) == 0ull) atomicAdd(st.started, 1u);
+                    }
                     j = c;
                     atomicAdd(&r.pending, 1);  // token: the job cannot complete mid make_work
-                    if (r.t_admit == 0ull) r.t_admit = global_ns();
                     break;
                 }
             }

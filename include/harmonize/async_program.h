@@ -13,8 +13,9 @@
 //
 // Internals (the B200 design, not a translation):
 //  * a "team" is one warp; a CTA holds TEAMS_PER_CTA teams. Each team owns, in shared
-//    memory, one ring per async function of RING_LINKS*32 promise slots, stored as
-//    structure-of-arrays 32-bit words (conflict-free for 32 consecutive slots).
+//    memory, one ring per async function of RING_LINKS*32 promise slots (a spec may size
+//    functions' rings apart with RING_LINKS_OF<Op>), stored as structure-of-arrays 32-bit
+//    words (conflict-free for 32 consecutive slots).
 //  * prog.async<F>: the lanes active at the call site reserve slots with ONE shared-memory
 //    atomicAdd issued by the lowest lane (__activemask / popc rank / __shfl_sync), then each
 //    lane writes its own words. Promises of one function therefore land contiguously, and
@@ -80,6 +81,8 @@ class AsyncProgram {
     static const unsigned int TEAMS_PER_CTA = (unsigned int)hrm_rt::spec_TEAMS_PER_CTA<PROGRAM_SPEC>::value;
     static const unsigned int CTA_THREADS = TEAMS_PER_CTA * 32u;
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
+    static const unsigned int COALESCE_PATIENCE =
+        (unsigned int)hrm_rt::spec_COALESCE_PATIENCE<PROGRAM_SPEC>::value;
 
     static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
     static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
@@ -94,6 +97,44 @@ class AsyncProgram {
     static const unsigned int TOTAL_WORDS = Layout::TOTAL_WORDS;
     static const unsigned int LINK_WORDS = Layout::MAX_WORDS;  // words per promise in a link
 
+    // Ring geometry: function F's ring holds ring_slots<F>() promises (RING_LINKS, or the
+    // spec's RING_LINKS_OF<Op>, links of 32), and word i of its slot s is stored at
+    // words[ring_base<F>() + i * ring_slots<F>() + s] of the team's stash.
+    template <unsigned int F>
+    __host__ __device__ static constexpr unsigned int ring_slots() {
+        using Op = typename OpAt<F, OpSet>::type;
+        return (unsigned int)hrm_rt::fn_RING_LINKS<PROGRAM_SPEC, Op>::value * 32u;
+    }
+    template <unsigned int F>
+    __host__ __device__ static constexpr unsigned int ring_base() {
+        if constexpr (F == 0) {
+            return 0u;
+        } else {
+            using Op = typename OpAt<F - 1, OpSet>::type;
+            return ring_base<F - 1>() + Promise<Op>::WORDS * ring_slots<F - 1>();
+        }
+    }
+    template <unsigned int I>
+    __host__ __device__ static constexpr bool rings_valid() {
+        if constexpr (I < FN) {
+            constexpr unsigned int s = ring_slots<I>();
+            return s >= 64u && (s & (s - 1u)) == 0u && rings_valid<I + 1>();
+        } else {
+            return true;
+        }
+    }
+    static_assert(rings_valid<0>(), "ring sizes must be powers of two of at least 2 links");
+    static const unsigned int RING_WORDS = ring_base<FN>();
+    // Ring size of function f (run-time f).
+    template <unsigned int I = 0>
+    __device__ static __forceinline__ unsigned int ring_slots_of(unsigned int f) {
+        if constexpr (I < FN) {
+            return f == I ? ring_slots<I>() : ring_slots_of<I + 1>(f);
+        } else {
+            return 0u;
+        }
+    }
+
     // -----------------------------------------------------------------------------------
     // Contexts (the names of async.h:181-262; contents are this runtime's).
     // -----------------------------------------------------------------------------------
@@ -102,11 +143,11 @@ class AsyncProgram {
         unsigned int rand_state;
     };
 
-    // One team's shared-memory stash: a ring of RING promise slots per function.
+    // One team's shared-memory stash: one ring of promise slots per function.
     struct GroupContext {
-        unsigned int count[FN];    // promises held per function (may exceed RING briefly)
+        unsigned int count[FN];    // promises held per function (may exceed the ring briefly)
         unsigned int bottom[FN];   // ring index of the oldest promise per function
-        unsigned int words[TOTAL_WORDS][RING];
+        unsigned int words[RING_WORDS];
     };
 
     struct DeviceContext {
@@ -319,7 +360,8 @@ class AsyncProgram {
     __device__ __forceinline__ void push_promise(const Promise<TYPE>& p) {
         constexpr unsigned int F = disc_of<TYPE>();
         constexpr unsigned int W = Promise<TYPE>::WORDS;
-        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        constexpr unsigned int SLOTS = ring_slots<F>();
+        constexpr unsigned int BASE = ring_base<F>();
         unsigned int w[W];
         p.to_words(w);
         const unsigned int mask = __activemask();
@@ -330,21 +372,22 @@ class AsyncProgram {
         if (rank == 0) base = atomicAdd(&g.count[F], (unsigned int)__popc(mask));
         base = __shfl_sync(mask, base, leader);
         const unsigned int idx = base + rank;
-        const unsigned int over = __ballot_sync(mask, idx >= RING);
-        if (idx < RING) {
-            const unsigned int slot = (g.bottom[F] + idx) & (RING - 1);
+        const unsigned int over = __ballot_sync(mask, idx >= SLOTS);
+        if (idx < SLOTS) {
+            const unsigned int slot = (g.bottom[F] + idx) & (SLOTS - 1);
 #pragma unroll
-            for (unsigned int i = 0; i < W; i++) g.words[OFF + i][slot] = w[i];
+            for (unsigned int i = 0; i < W; i++) g.words[BASE + i * SLOTS + slot] = w[i];
         }
-        if (over != 0 && idx >= RING) {
+        if (over != 0 && idx >= SLOTS) {
             overflow_to_arena<TYPE>(w, over);
         }
     }
 
     // Lanes in `over` could not fit in shared memory: write them straight to one arena link
-    // and publish it to the function's queue.
+    // and publish it to the function's queue. (Inlined so that the promise words stay in
+    // registers: a call taking them by reference would put every push's words on the stack.)
     template <typename TYPE>
-    __device__ __noinline__ void overflow_to_arena(const unsigned int (&w)[Promise<TYPE>::WORDS], unsigned int over) {
+    __device__ __forceinline__ void overflow_to_arena(const unsigned int (&w)[Promise<TYPE>::WORDS], unsigned int over) {
         constexpr unsigned int F = disc_of<TYPE>();
         constexpr unsigned int W = Promise<TYPE>::WORDS;
         const unsigned int r = __popc(over & util::lanemask_lt());
@@ -431,7 +474,8 @@ class AsyncProgram {
     __device__ void spill_typed(unsigned int nlinks, unsigned long long& spilled) {
         using Op = typename OpAt<F, OpSet>::type;
         constexpr unsigned int W = Promise<Op>::WORDS;
-        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        constexpr unsigned int SLOTS = ring_slots<F>();
+        constexpr unsigned int BASE = ring_base<F>();
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         unsigned int cnt = g.count[F];
@@ -450,9 +494,9 @@ class AsyncProgram {
             unsigned int dst = __shfl_sync(0xFFFFFFFFu, link, l);
             unsigned int k = l * 32u + lane;
             if (k < n) {
-                unsigned int slot = (bottom + k) & (RING - 1);
+                unsigned int slot = (bottom + k) & (SLOTS - 1);
 #pragma unroll
-                for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(dst, i, lane), g.words[OFF + i][slot]);
+                for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(dst, i, lane), g.words[BASE + i * SLOTS + slot]);
             }
         }
         __threadfence();
@@ -461,7 +505,7 @@ class AsyncProgram {
         hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, cnt_l), lane, nl, 0xFFFFFFFFu);
         __syncwarp();
         if (lane == 0) {
-            g.bottom[F] = (bottom + n) & (RING - 1);
+            g.bottom[F] = (bottom + n) & (SLOTS - 1);
             g.count[F] = cnt - n;
         }
         __syncwarp();
@@ -482,11 +526,12 @@ class AsyncProgram {
     __device__ unsigned int fill_typed() {
         using Op = typename OpAt<F, OpSet>::type;
         constexpr unsigned int W = Promise<Op>::WORDS;
-        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        constexpr unsigned int SLOTS = ring_slots<F>();
+        constexpr unsigned int BASE = ring_base<F>();
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         unsigned int cnt = g.count[F];
-        unsigned int room = (RING - cnt) / 32u;   // links that surely fit
+        unsigned int room = (SLOTS - cnt) / 32u;   // links that surely fit
         unsigned int want = min(room, 2u);
         if (want == 0) return 0;
         unsigned int pos = 0, take = 0;
@@ -504,9 +549,9 @@ class AsyncProgram {
             unsigned int src = hrm_rt::entry_link(el);
             unsigned int k = hrm_rt::entry_count(el);
             if (lane < k) {
-                unsigned int slot = (bottom + cnt + lane) & (RING - 1);
+                unsigned int slot = (bottom + cnt + lane) & (SLOTS - 1);
 #pragma unroll
-                for (unsigned int i = 0; i < W; i++) g.words[OFF + i][slot] = __ldcg(link_word_ptr(src, i, lane));
+                for (unsigned int i = 0; i < W; i++) g.words[BASE + i * SLOTS + slot] = __ldcg(link_word_ptr(src, i, lane));
             }
             cnt += k;
         }
@@ -535,16 +580,17 @@ class AsyncProgram {
     __device__ __forceinline__ void run_typed(unsigned int k) {
         using Op = typename OpAt<F, OpSet>::type;
         constexpr unsigned int W = Promise<Op>::WORDS;
-        constexpr unsigned int OFF = OpWordOffset<F, OpSet>::value;
+        constexpr unsigned int SLOTS = ring_slots<F>();
+        constexpr unsigned int BASE = ring_base<F>();
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         const unsigned int cnt = g.count[F];
         Promise<Op> p;
         if (lane < k) {
             unsigned int w[W];
-            unsigned int slot = (g.bottom[F] + cnt - k + lane) & (RING - 1);
+            unsigned int slot = (g.bottom[F] + cnt - k + lane) & (SLOTS - 1);
 #pragma unroll
-            for (unsigned int i = 0; i < W; i++) w[i] = g.words[OFF + i][slot];
+            for (unsigned int i = 0; i < W; i++) w[i] = g.words[BASE + i * SLOTS + slot];
             p.from_words(w);
         }
         __syncwarp();
@@ -564,13 +610,14 @@ class AsyncProgram {
         }
     }
 
-    // Counts above RING mean the excess went to the arena: clamp.
+    // Counts above the ring size mean the excess went to the arena: clamp.
     __device__ __forceinline__ void clamp_counts() {
         __syncwarp();
         const unsigned int lane = util::lane_id();
         if (lane < FN) {
+            const unsigned int slots = ring_slots_of(lane);
             unsigned int c = _grp_ctx.count[lane];
-            if (c > RING) _grp_ctx.count[lane] = RING;
+            if (c > slots) _grp_ctx.count[lane] = slots;
         }
         __syncwarp();
     }
@@ -633,7 +680,10 @@ class AsyncProgram {
         unsigned int backoff = 32;
         unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_spill = 0, n_fill = 0, n_mw = 0, n_idle = 0;
         unsigned long long fn_evals = 0;  // lane f counts the evaluations of function f
+        unsigned int patience = 0;        // steps scheduled while some function held partial work
+        unsigned int rotate = 0;          // next function to favour for a patience-forced batch
         bool quiescent = false;
+        const unsigned int my_ring = (lane < FN) ? ring_slots_of(lane) : 0u;  // lane f: f's ring size
 
         for (unsigned int cycle = 0; cycle < cycle_count; cycle++) {
             // Stop on a halt request or an error flag.
@@ -650,7 +700,22 @@ class AsyncProgram {
             unsigned int best = __reduce_max_sync(0xFFFFFFFFu, key);
             unsigned int bf = best & 31u, bc = best >> 5;
 
-            if (bc < 32u) {
+            bool forced = false;
+            const unsigned int partial = __ballot_sync(0xFFFFFFFFu, lane < FN && c > 0u && c < 32u);
+            if (partial != 0u && ++patience >= COALESCE_PATIENCE) {
+                // Some function holds a partial batch and the team has passed it over
+                // COALESCE_PATIENCE times (for full batches of other functions, arena fills
+                // or make_work): run one partial batch now, taking the partial functions in
+                // turn, so that no promise waits without bound behind a steady supply of
+                // other work (e.g. the last Collatz steps of a small job among photon jobs).
+                patience = 0;
+                rotate = (rotate + 1u) % FN;
+                const unsigned int upper = partial >> rotate;
+                bf = upper ? rotate + (unsigned int)(__ffs(upper) - 1) : (unsigned int)(__ffs(partial) - 1);
+                bc = __shfl_sync(0xFFFFFFFFu, c, bf);
+                forced = true;
+            }
+            if (bc < 32u && !forced) {
                 // No full batch locally: try the arena for the function closest to full.
                 unsigned int av = 0;
                 if (lane < FN) av = hrm_rt::ld_relaxed(&_dev_ctx.rings.heads[lane].avail);
@@ -690,6 +755,8 @@ class AsyncProgram {
                 }
                 if (bc == 0) {
                     // Nothing local, nothing in the arena, nothing to make: idle.
+                    hrm_rt::call_on_idle<PROGRAM_SPEC>(*this);
+                    __syncwarp();
                     unsigned int st = 0;
                     if (lane == 0) st = idle_poll(counted_idle, backoff);
                     st = __shfl_sync(0xFFFFFFFFu, st, 0);
@@ -708,14 +775,16 @@ class AsyncProgram {
             unsigned int k = min(bc, 32u);
             // Every other ring needs one link of headroom for the calls this batch makes
             // (the batch's own ring frees k slots when it is popped).
-            unsigned int hi = __ballot_sync(0xFFFFFFFFu, lane < FN && lane != bf && c > RING - 32u);
+            unsigned int hi = __ballot_sync(0xFFFFFFFFu, lane < FN && lane != bf && c > my_ring - 32u);
             while (hi) {
                 unsigned int f = __ffs(hi) - 1;
                 hi &= hi - 1;
                 unsigned int cf = __shfl_sync(0xFFFFFFFFu, c, f);
-                spill_fn<0>(f, (cf - (RING - 32u) + 31u) / 32u, n_spill);
+                unsigned int rf = __shfl_sync(0xFFFFFFFFu, my_ring, f);
+                spill_fn<0>(f, (cf - (rf - 32u) + 31u) / 32u, n_spill);
             }
             run_fn<0>(bf, k);
+            hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
             clamp_counts();
             n_evals += k;
             n_batches += 1;

@@ -48,9 +48,23 @@ HRM_SPEC_CONST(GROUP_SIZE, 32)
 HRM_SPEC_CONST(RING_LINKS, 2)      // per-function shared-memory ring, in 32-promise links
 HRM_SPEC_CONST(TEAMS_PER_CTA, 4)   // 32-lane teams (work groups) per CTA
 HRM_SPEC_CONST(MIN_CTAS_PER_SM, 1) // occupancy hint for __launch_bounds__
+// Coalescing threshold: while some function holds a partial batch (1-31 promises), a team
+// schedules at most this many other steps (full batches of other functions, arena fills,
+// make_work calls) before it runs one partial batch (partial functions taken in turn), so
+// that no promise waits behind an endless supply of other work.
+HRM_SPEC_CONST(COALESCE_PATIENCE, 8)
 
 #undef HRM_SPEC_TYPE
 #undef HRM_SPEC_CONST
+
+// Per-function ring size: a spec may give functions rings of different sizes by defining
+//   template <typename Op> struct RING_LINKS_OF { static const size_t value = ...; };
+// (a power of two >= 2 for each Op); otherwise every function gets RING_LINKS.
+template <class S, class Op, class = void>
+struct fn_RING_LINKS : spec_RING_LINKS<S> {};
+template <class S, class Op>
+struct fn_RING_LINKS<S, Op, std::void_t<decltype(S::template RING_LINKS_OF<Op>::value)>>
+    : std::integral_constant<size_t, (size_t)(S::template RING_LINKS_OF<Op>::value)> {};
 
 template <class S, class P, class = void>
 struct has_initialize : std::false_type {};
@@ -85,6 +99,31 @@ __device__ __forceinline__ bool call_make_work(P prog) {
     } else {
         return false;
     }
+}
+
+// Optional hooks of this runtime's AsyncProgram (no counterpart in the original API), for
+// specs that keep per-team bookkeeping in their GroupState:
+//   template <class P> __device__ static void after_batch(P prog);
+//     called by the whole team, converged, right after the evaluations of each batch;
+//   template <class P> __device__ static void on_idle(P prog);
+//     called by the whole team when it finds no work at all, before it waits, so that
+//     bookkeeping held by the team is published before the team sleeps.
+template <class S, class P, class = void>
+struct has_on_idle : std::false_type {};
+template <class S, class P>
+struct has_on_idle<S, P, std::void_t<decltype(S::template on_idle<P>(std::declval<P>()))>> : std::true_type {};
+template <class S, class P>
+__device__ __forceinline__ void call_on_idle(P prog) {
+    if constexpr (has_on_idle<S, P>::value) S::template on_idle<P>(prog);
+}
+template <class S, class P, class = void>
+struct has_after_batch : std::false_type {};
+template <class S, class P>
+struct has_after_batch<S, P, std::void_t<decltype(S::template after_batch<P>(std::declval<P>()))>>
+    : std::true_type {};
+template <class S, class P>
+__device__ __forceinline__ void call_after_batch(P prog) {
+    if constexpr (has_after_batch<S, P>::value) S::template after_batch<P>(prog);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -182,7 +221,7 @@ enum StatIndex : unsigned int {
 // t waits for sequence t, writes {t+1, entry}; a consumer owning position t waits for
 // sequence t+1 and writes {t+capacity, 0}. Positions are handed out in batches by one
 // atomicAdd per warp. `avail` counts published, unclaimed entries; a consumer first
-// reserves entries from `avail` (compare-and-swap), then positions from `head`.
+// reserves entries from `avail` (atomicSub, see ring_reserve), then positions from `head`.
 // ---------------------------------------------------------------------------------------
 struct alignas(128) RingHead {
     unsigned int head;

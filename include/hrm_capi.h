@@ -183,6 +183,28 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
 int hrm_bfs_run_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32_t root,
                        uint32_t* d_levels, const hrm_run_config* cfg, hrm_run_result* res);
 
+/* Remapping-barrier workload (harmonize examples/cpp/barrier_demo/demo.cpp:20-86, which the
+ * original runs as `demo dep=.. ndep=.. bar=..`): ids [0, dep+ndep) each run one Step; the
+ * dependent ones (id < dep) hold a follow-up Step on RemappingBarrier id % bar and then
+ * decrement it, each barrier starting at the number of dependent ids mapped to it; a
+ * UnitBarrier armed with ndep releases one final Step after the non-dependent Steps.
+ * counter[4] (host) receives: Steps run (2*dep + ndep + (ndep > 0)), non-dependent Steps,
+ * final Steps, and violations (a follow-up that ran before its barrier released, or a final
+ * Step that ran early; always 0). released[bar] (host) receives the follow-ups run per
+ * barrier. AsyncProgram only (barriers keep held promises in the arena); bar >= 1. */
+int hrm_barrier_demo_run(uint32_t dep_count, uint32_t non_dep_count, uint32_t barrier_count, uint32_t* counter,
+                         uint32_t* released, const hrm_run_config* cfg, hrm_run_result* res);
+
+/* Device state of HRM_SPEC_BARRIER_DEMO for hrm_program_create (device pointers). */
+typedef struct hrm_barrier_demo_state {
+    uint32_t dep_count, non_dep_count, barrier_count, pad;
+    void* source;              /* AtomicIter<uint32> over [0, dep + ndep) */
+    uint32_t* counter;         /* 4 counters, zeroed */
+    uint32_t* released;        /* barrier_count counters, zeroed */
+    void* barriers;            /* barrier_count RemappingBarrier values made by blank(wait count) */
+    void* unit;                /* one UnitBarrier */
+} hrm_barrier_demo_state;
+
 /* ---- many independent jobs --------------------------------------------------------------
  * No counterpart in the original (one program instance per launch there). A job is one
  * instance of a built-in spec; all pointers are device pointers owned by the caller. */

@@ -109,3 +109,13 @@ def test_bfs_edge_cases():
     assert list(oracle.bfs(rp, col, 0)) == [0, 1, 2]
     lv, _ = oracle.exec_bfs(rp, col, 0)
     assert list(lv) == [0, 1, 2]
+
+
+def test_barrier_oracle_counts():
+    from oracle.barrier import barrier_demo
+    for dep, ndep, bar in [(0, 1, 1), (10, 3, 3), (1000, 17, 7), (5, 0, 9)]:
+        counter, released = barrier_demo(dep, ndep, bar)
+        # demo.cpp:216 expects dep*2 + ndep Steps; the unit barrier adds one final Step.
+        assert counter == [2 * dep + ndep + (1 if ndep else 0), ndep, 1 if ndep else 0, 0]
+        assert released == [dep // bar + (1 if dep % bar > b else 0) for b in range(bar)]
+        assert sum(released) == dep
