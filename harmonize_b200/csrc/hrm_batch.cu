@@ -178,13 +178,18 @@ struct Batch : BatchBase {
     }
     JobRecord* table() override { return jobs.data(); }
 
-    // Captures: timestamp, output preparation, init<P>, exec<P>.
-    void capture(size_t groups, size_t cycles) {
-        if (graph && groups == graph_groups && cycles == graph_cycles) return;
+    // Captures: timestamp, output preparation, init<P>, exec<P> (the launches bake in the
+    // instance's tunables, so a change of them re-captures).
+    void capture(size_t groups, size_t cycles, unsigned int patience, unsigned int fill_links) {
+        if (graph && groups == graph_groups && cycles == graph_cycles && patience == inst.patience &&
+            fill_links == inst.fill_links)
+            return;
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
         }
+        inst.patience = patience;
+        inst.fill_links = fill_links;
         P::resident_ctas();  // sets the kernel's shared-memory attribute outside the capture
         cudaGraph_t g;
         ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -206,7 +211,7 @@ struct Batch : BatchBase {
         size_t groups = cfg.groups ? cfg.groups : (size_t)1 << 30;
         size_t cycles = cfg.cycles ? cfg.cycles : ((size_t)1 << 24);
         size_t max_execs = cfg.max_execs ? cfg.max_execs : 4096;
-        capture(groups, cycles);
+        capture(groups, cycles, cfg.patience, cfg.fill_links);
         unsigned int ctr[8] = {n, 0u, 0u, 0u, closed0, 0u, 0u, 0u};
         ck(cudaMemcpyAsync(jobs.data(), recs.data(), sizeof(JobRecord) * n, cudaMemcpyHostToDevice, stream), "jobs");
         ck(cudaMemcpyAsync(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice, stream), "counters");
@@ -397,6 +402,8 @@ struct Server : ServerBase {
         MixState st = Batch<P>::state_for(jobs.data(), counters.data(), cap);
         st.done_host = done_dev;
         inst.device_state = st;
+        inst.patience = cfg.patience;
+        inst.fill_links = cfg.fill_links;
         unsigned int ctr[8] = {0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
         ck(cudaMemcpy(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice), "counters");
         P::launch_init(inst, groups, exec_s);
@@ -773,6 +780,48 @@ int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg
         return hrm_capi::set_error(HRM_EINVAL, e.what());
     } catch (std::exception& e) {
         return hrm_capi::set_error(HRM_EDEVICE, e.what());
+    }
+}
+
+int hrm_runtime_run(const hrm_job* jobs, uint32_t njobs, int program_type, const int* variants, uint64_t* done_ns,
+                    float* total_ms) {
+    if (jobs == nullptr && njobs != 0) return hrm_capi::set_error(HRM_EINVAL, "jobs is NULL");
+    try {
+        for (uint32_t j = 0; j < njobs; j++) validate(jobs[j]);
+        ck(cudaDeviceSynchronize(), "sync");
+        auto t0 = std::chrono::steady_clock::now();
+        for (uint32_t j = 0; j < njobs; j++) {
+            const hrm_job& jb = jobs[j];
+            hrm_run_config cfg;
+            memset(&cfg, 0, sizeof(cfg));
+            cfg.program_type = program_type;
+            cfg.variant = variants ? variants[jb.kind] : 0;
+            hrm_run_result res;
+            int rc = HRM_OK;
+            if (jb.kind == HRM_JOB_COLLATZ) {
+                rc = hrm_collatz_run_device(jb.first, jb.count, (uint32_t*)jb.out, &cfg, &res);
+            } else if (jb.kind == HRM_JOB_PHOTON) {
+                rc = hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
+                                           jb.first, jb.count, (uint64_t*)jb.out, &cfg, &res);
+            } else {
+                rc = hrm_bfs_run_device((const uint32_t*)jb.a, (const uint32_t*)jb.b, jb.n, jb.first,
+                                        (uint32_t*)jb.out, &cfg, &res);
+            }
+            if (rc != HRM_OK) return rc;  // message already set by the whole-run call
+            if (done_ns) {
+                done_ns[j] = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                 std::chrono::steady_clock::now() - t0)
+                                 .count();
+            }
+        }
+        if (total_ms) {
+            *total_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_ECUDA, e.what());
     }
 }
 

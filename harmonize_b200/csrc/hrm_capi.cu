@@ -49,6 +49,7 @@ struct ProgramBase {
     virtual std::vector<unsigned long long> stats() = 0;
     virtual std::vector<unsigned int> overview() = 0;
     virtual void set_state(const void* state, size_t size) = 0;
+    virtual void set_tuning(unsigned int patience, unsigned int fill_links) = 0;
     // Device scratch of the whole-run helpers (the start-value / source iterator), kept with
     // the instance so that cached runs allocate nothing.
     util::host::DevBuf<util::iter::AtomicIter<unsigned int>> iterator{(size_t)1};
@@ -75,6 +76,12 @@ struct ProgramImpl : ProgramBase {
     void set_state(const void* state, size_t size) override {
         if (size != sizeof(typename P::DeviceState)) throw std::invalid_argument("device state size mismatch");
         memcpy((void*)&inst.device_state, state, size);
+    }
+    void set_tuning(unsigned int patience, unsigned int fill_links) override {
+        if constexpr (hrm_capi::is_async_program<P>::value) {
+            inst.patience = patience;
+            inst.fill_links = fill_links;
+        }
     }
 };
 
@@ -172,6 +179,7 @@ int run_to_completion(ProgramBase* p, const hrm_run_config& cfg, hrm_run_result*
     ck(cudaEventCreate(&e0), "cudaEventCreate");
     ck(cudaEventCreate(&e1), "cudaEventCreate");
     ck(cudaEventRecord(e0, s), "cudaEventRecord");
+    p->set_tuning(cfg.patience, cfg.fill_links);
     p->init(groups, s);
     ck(cudaGetLastError(), "init launch");
     size_t execs = 0;

@@ -269,7 +269,10 @@ struct Job {
     HRM_DEV static void eval(PROGRAM prog, unsigned int job, A... a) {
         using S = typename JobStateOf<F>::type;
         const MixState& st = prog.device;
-        S& inner_state = JobStateOf<F>::get(st.jobs[job]);
+        // A copy in registers: the inner evals only read their state (the pointers in it
+        // lead to the job's buffers), and a register copy saves re-loading the job record
+        // after every store the eval makes.
+        S inner_state = JobStateOf<F>::get(st.jobs[job]);
         int delta = -1;
         JobProgram<PROGRAM, S> jp{prog, inner_state, job, &delta};
         F::template eval<JobProgram<PROGRAM, S>>(jp, a...);
@@ -300,9 +303,11 @@ HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int 
     return delta;
 }
 
-// RING: ring links of the two photon functions whose promises carry a whole photon (move,
-// collide: 12 words each); every other function (5 words or fewer) gets 2 links, which
-// keeps a team's stash small enough for 12-16 resident teams per SM.
+// RING: ring links of the photon functions (move and collide carry a whole photon, 12
+// words; every collide batch feeds a batch of tallies, so each needs room for several
+// batches). Collatz and BFS functions get 2 links: a Collatz step makes one successor and
+// a BFS expansion overflows to the arena whatever the ring, so small rings cost them little
+// and keep a team's stash small (more resident teams per SM).
 template <size_t RING = 4, size_t TEAMS = 4>
 struct MixSpec {
     typedef OpUnion<Job<CollatzEven>, Job<CollatzOdd>, Job<PhotonMove>, Job<PhotonCollide>, Job<PhotonTally>,
@@ -316,8 +321,11 @@ struct MixSpec {
     static const size_t TEAMS_PER_CTA = TEAMS;
     template <typename Op>
     struct RING_LINKS_OF {
-        static const size_t value =
-            (std::is_same<Op, Job<PhotonMove>>::value || std::is_same<Op, Job<PhotonCollide>>::value) ? RING : 2;
+        static const size_t value = (std::is_same<Op, Job<PhotonMove>>::value ||
+                                     std::is_same<Op, Job<PhotonCollide>>::value ||
+                                     std::is_same<Op, Job<PhotonTally>>::value)
+                                        ? RING
+                                        : 2;
     };
 
     template <typename PROGRAM>

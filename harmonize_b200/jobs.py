@@ -33,6 +33,9 @@ def _bind():
         L.hrm_batch_run.restype = ctypes.c_int
         L.hrm_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]
+        L.hrm_runtime_run.restype = ctypes.c_int
+        L.hrm_runtime_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
         L.hrm_plain_run.restype = ctypes.c_int
         L.hrm_plain_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                     ctypes.POINTER(ctypes.c_float)]
@@ -105,10 +108,10 @@ def poisson_arrivals(n, rate_per_s, seed=11):
 
 
 class Mix:
-    """A list of jobs with their device inputs and two sets of device outputs (so that a
-    batched run and a plain run can be compared)."""
+    """A list of jobs with their device inputs and `sets` sets of device outputs (so that a
+    batched run and baseline runs can be compared)."""
 
-    def __init__(self, specs, photon_grid=32, media=8, seed=1):
+    def __init__(self, specs, photon_grid=32, media=8, seed=1, sets=2):
         import torch
         self.torch = torch
         # list of dicts: kind, first, count / scale, medium / graph index
@@ -124,7 +127,7 @@ class Mix:
                 rp, col = rmat_csr(s["scale"], 16, 0.57, 0.19, 0.19, seed * 100 + s["scale"])
                 self.graphs[s["scale"]] = (torch.from_numpy(rp.view(np.int32)).cuda(),
                                            torch.from_numpy(col.view(np.int32)).cuda(), rp, col)
-        self.outputs = [self._alloc_outputs(), self._alloc_outputs()]
+        self.outputs = [self._alloc_outputs() for _ in range(sets)]
 
     def _alloc_outputs(self):
         torch = self.torch
@@ -193,6 +196,23 @@ def batch_run(mix, which=0, indices=None, **cfg_kw):
     res = RunResult()
     check(L.hrm_batch_run(ctypes.byref(arr), len(arr), ctypes.byref(cfg), ctypes.byref(res), done.ctypes.data))
     return done, res.as_dict()
+
+
+def runtime_run(mix, which=1, indices=None, program="async", variants=None):
+    """One whole single-spec runtime run per job, in order (plain execution of the runtime).
+    variants: per job kind (Collatz, photon, BFS), default the autotuner's choice for each.
+    Returns (done_ns array, total ms)."""
+    L = _bind()
+    arr = mix.job_array(which, indices)
+    done = np.zeros(len(arr), dtype=np.uint64)
+    total = ctypes.c_float()
+    if variants is None:
+        from .autotune import tuned_variant
+        variants = [tuned_variant(w, program) for w in ("collatz", "photon", "bfs")]
+    v = (ctypes.c_int * 3)(*variants)
+    pt = {"async": 0, "event": 1}[program]
+    check(L.hrm_runtime_run(ctypes.byref(arr), len(arr), pt, v, done.ctypes.data, ctypes.byref(total)))
+    return done, total.value
 
 
 def plain_run(mix, which=1, indices=None, streams=16):

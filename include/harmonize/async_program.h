@@ -158,6 +158,8 @@ class AsyncProgram {
         unsigned int* link_meta;      // per link {next + 1, promise count}; used by barriers
         unsigned long long* stats;    // hrm_rt::STAT_COUNT counters
         unsigned int arena_links;
+        unsigned int patience;        // coalescing threshold in force (COALESCE_PATIENCE by default)
+        unsigned int fill_links;      // links one fill may take from a queue (2 by default)
     };
 
     // -----------------------------------------------------------------------------------
@@ -174,6 +176,9 @@ class AsyncProgram {
         unsigned int ring_capacity;
         DeviceState device_state;
         cudaStream_t stream = nullptr;
+        // Run-time tunables (0 = the spec's default): see DeviceContext.
+        unsigned int patience = 0;
+        unsigned int fill_links = 0;
 
         __host__ Instance(AdrType arsize, DeviceState ds)
             : arena_size(arsize),
@@ -202,6 +207,8 @@ class AsyncProgram {
             c.link_meta = link_meta.data();
             c.stats = stats.data();
             c.arena_links = (unsigned int)arena_size;
+            c.patience = patience ? patience : COALESCE_PATIENCE;
+            c.fill_links = fill_links ? (fill_links < 32u ? fill_links : 32u) : 2u;
             return c;
         }
 
@@ -532,7 +539,7 @@ class AsyncProgram {
         const unsigned int lane = util::lane_id();
         unsigned int cnt = g.count[F];
         unsigned int room = (SLOTS - cnt) / 32u;   // links that surely fit
-        unsigned int want = min(room, 2u);
+        unsigned int want = min(room, _dev_ctx.fill_links);
         if (want == 0) return 0;
         unsigned int pos = 0, take = 0;
         if (lane == 0) take = hrm_rt::ring_reserve(_dev_ctx.rings, F, want, pos);
@@ -680,8 +687,9 @@ class AsyncProgram {
         unsigned int backoff = 32;
         unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_spill = 0, n_fill = 0, n_mw = 0, n_idle = 0;
         unsigned long long fn_evals = 0;  // lane f counts the evaluations of function f
-        unsigned int patience = 0;        // steps scheduled while some function held partial work
-        unsigned int rotate = 0;          // next function to favour for a patience-forced batch
+        unsigned int prev_c = 0;          // lane f: f's count at the previous step
+        unsigned int age = 0;             // lane f: steps f has held a partial batch that did not grow
+        unsigned int rotate = 0;          // next function to favour for a forced partial batch
         bool quiescent = false;
         const unsigned int my_ring = (lane < FN) ? ring_slots_of(lane) : 0u;  // lane f: f's ring size
 
@@ -700,19 +708,24 @@ class AsyncProgram {
             unsigned int best = __reduce_max_sync(0xFFFFFFFFu, key);
             unsigned int bf = best & 31u, bc = best >> 5;
 
+            // A partial batch that stops growing is starving: other work (full batches of
+            // other functions, fills, make_work) keeps the team busy and nothing will top it
+            // up. After `patience` such steps run it anyway, starving functions taken
+            // in turn, so that no promise waits without bound (e.g. the last Collatz steps of
+            // a small job among photon jobs). A partial batch that keeps growing (photon
+            // tallies fed by every collide batch) is left to fill up.
+            if (lane < FN) {
+                age = (c > 0u && c < 32u && c <= prev_c) ? age + 1u : 0u;
+                prev_c = c;
+            }
             bool forced = false;
-            const unsigned int partial = __ballot_sync(0xFFFFFFFFu, lane < FN && c > 0u && c < 32u);
-            if (partial != 0u && ++patience >= COALESCE_PATIENCE) {
-                // Some function holds a partial batch and the team has passed it over
-                // COALESCE_PATIENCE times (for full batches of other functions, arena fills
-                // or make_work): run one partial batch now, taking the partial functions in
-                // turn, so that no promise waits without bound behind a steady supply of
-                // other work (e.g. the last Collatz steps of a small job among photon jobs).
-                patience = 0;
+            const unsigned int starving = __ballot_sync(0xFFFFFFFFu, lane < FN && age >= _dev_ctx.patience);
+            if (starving != 0u) {
                 rotate = (rotate + 1u) % FN;
-                const unsigned int upper = partial >> rotate;
-                bf = upper ? rotate + (unsigned int)(__ffs(upper) - 1) : (unsigned int)(__ffs(partial) - 1);
+                const unsigned int upper = starving >> rotate;
+                bf = upper ? rotate + (unsigned int)(__ffs(upper) - 1) : (unsigned int)(__ffs(starving) - 1);
                 bc = __shfl_sync(0xFFFFFFFFu, c, bf);
+                if (lane == bf) age = 0;
                 forced = true;
             }
             if (bc < 32u && !forced) {

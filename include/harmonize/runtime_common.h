@@ -48,11 +48,11 @@ HRM_SPEC_CONST(GROUP_SIZE, 32)
 HRM_SPEC_CONST(RING_LINKS, 2)      // per-function shared-memory ring, in 32-promise links
 HRM_SPEC_CONST(TEAMS_PER_CTA, 4)   // 32-lane teams (work groups) per CTA
 HRM_SPEC_CONST(MIN_CTAS_PER_SM, 1) // occupancy hint for __launch_bounds__
-// Coalescing threshold: while some function holds a partial batch (1-31 promises), a team
-// schedules at most this many other steps (full batches of other functions, arena fills,
-// make_work calls) before it runs one partial batch (partial functions taken in turn), so
-// that no promise waits behind an endless supply of other work.
-HRM_SPEC_CONST(COALESCE_PATIENCE, 8)
+// Coalescing threshold: a function whose partial batch (1-31 promises) has not grown for
+// this many scheduling steps of its team (full batches of other functions, arena fills,
+// make_work calls) is run as a partial batch, so that no promise waits behind an endless
+// supply of other work, while partial batches that are still filling are left to fill.
+HRM_SPEC_CONST(COALESCE_PATIENCE, 16)
 
 #undef HRM_SPEC_TYPE
 #undef HRM_SPEC_CONST

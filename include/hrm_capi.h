@@ -76,6 +76,9 @@ typedef struct hrm_run_config {
     size_t max_execs;          /* exec calls before giving up with HRM_EINCOMPLETE; 0 = 4096 */
     void* stream;              /* cudaStream_t, NULL = default stream */
     int variant;               /* compiled tuning variant (see HRM_VARIANT_*), 0 = default */
+    uint32_t patience;         /* AsyncProgram coalescing threshold: scheduling steps a partial
+                                  batch may wait without growing before it runs; 0 = 16 */
+    uint32_t fill_links;       /* AsyncProgram links one fill takes from the arena; 0 = 2 */
 } hrm_run_config;
 
 /* Compiled tuning variants: shared-memory ring per async function (in 32-promise links)
@@ -234,6 +237,13 @@ int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg
  * thread per source photon with its descendants, one CTA per BFS), jobs round-robin over
  * nstreams streams. done_ns as above; *total_ms = time until the last job completed. */
 int hrm_plain_run(const hrm_job* jobs, uint32_t njobs, uint32_t nstreams, uint64_t* done_ns, float* total_ms);
+/* Baseline: plain execution of the runtime itself, one job at a time, as a program built on
+ * the original would run them: for each job, one whole run of the single-spec program
+ * (hrm_collatz/photon/bfs_run_device: init, exec until complete, synchronised). variants
+ * (NULL = variant 0 for all) gives the compiled variant per job kind (HRM_JOB_*). done_ns
+ * (host clock, ns from the first job's start) and *total_ms as above. */
+int hrm_runtime_run(const hrm_job* jobs, uint32_t njobs, int program_type, const int* variants, uint64_t* done_ns,
+                    float* total_ms);
 
 /* ---- serving: a resident runtime admitting jobs while it runs ---------------------------
  * No counterpart in the original. hrm_server_open starts a persistent AsyncProgram over the

@@ -76,3 +76,25 @@ def test_inputs_are_deterministic(hrm):
     mu, ab, sp = hrm.photon_medium(64, 1)
     assert abs(np.log(mu).mean()) < 0.01 and abs(np.log(mu).std() - 0.5) < 0.01
     assert ab.min() >= 0.02 and ab.max() <= 0.2 and abs(sp.mean() - 0.1) < 0.01
+
+
+def test_ctypes_structs_match_the_c_layout(hrm, tmp_path):
+    """The Python mirrors of hrm_run_config / hrm_run_result / hrm_job have the C layout."""
+    from harmonize_b200 import jobs
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "hrm_capi.h"\n'
+                   'int main(void) {\n'
+                   '  printf("%zu %zu %zu %zu\\n", sizeof(hrm_run_config), offsetof(hrm_run_config, variant),\n'
+                   '         offsetof(hrm_run_config, patience), offsetof(hrm_run_config, fill_links));\n'
+                   '  printf("%zu %zu\\n", sizeof(hrm_run_result), offsetof(hrm_run_result, device_ms));\n'
+                   '  printf("%zu %zu\\n", sizeof(hrm_job), offsetof(hrm_job, out));\n'
+                   '  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [list(map(int, line.split())) for line in subprocess.check_output([str(exe)], text=True).splitlines()]
+    C = hrm.RunConfig
+    assert got[0] == [ctypes.sizeof(C), C.variant.offset, C.patience.offset, C.fill_links.offset]
+    assert got[1] == [ctypes.sizeof(hrm.RunResult), hrm.RunResult.device_ms.offset]
+    assert got[2] == [ctypes.sizeof(jobs.Job), jobs.Job.out.offset]
