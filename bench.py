@@ -131,18 +131,24 @@ def dist_setup(args):
     return rank, world, local, pg
 
 
+def _reduce_device(pg):
+    """Device of the reduction tensors: the GPU under NCCL, the CPU under gloo."""
+    return "cpu" if pg.get_backend() == "gloo" else "cuda"
+
+
 def barrier(pg):
     import torch
     if pg is not None:
         pg.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(pg, value):
     import torch
     if pg is None:
         return value
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -151,9 +157,14 @@ def sum_over_ranks(pg, value):
     import torch
     if pg is None:
         return value
-    t = torch.tensor([float(value)], dtype=torch.float64, device="cuda")
+    t = torch.tensor([float(value)], dtype=torch.float64, device=_reduce_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
+
+
+def replica_range(rank, count):
+    """Replicas only: rank r works on ids [r*count, (r+1)*count) (weak scaling, no exchange)."""
+    return rank * count, count
 
 
 def flush_l2(buf):
@@ -180,7 +191,7 @@ BYTES_PER_CALL = {
 def run_photon(args, hrm, rank, world, pg, torch):
     n = args.grid
     count = args.photons
-    first = rank * count
+    first, count = replica_range(rank, count)
     seed = 0x5EED0123456789
     mu, ab, sp = hrm.photon_medium(n, 2024)
     nvox = n ** 3
@@ -189,7 +200,7 @@ def run_photon(args, hrm, rank, world, pg, torch):
     d_ab = torch.from_numpy(ab).cuda()
     d_sp = torch.from_numpy(sp).cuda()
     d_tally = torch.zeros(slots, dtype=torch.int64, device="cuda")
-    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    cfg = hrm.make_config(args.program, **pick_config(args))
     L = hrm.lib()
 
     def step_device():
@@ -244,7 +255,7 @@ def run_bfs(args, hrm, rank, world, pg, torch):
     d_rp = torch.from_numpy(rp.view(np.int32)).cuda()
     d_col = torch.from_numpy(col.view(np.int32)).cuda()
     d_lev = torch.empty(nv, dtype=torch.int32, device="cuda")
-    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    cfg = hrm.make_config(args.program, **pick_config(args))
     L = hrm.lib()
 
     def step_device():
@@ -284,10 +295,10 @@ def run_bfs(args, hrm, rank, world, pg, torch):
 
 
 def run_collatz(args, hrm, rank, world, pg, torch):
-    count = 1 << 20
-    start = 1 + rank * count
+    first, count = replica_range(rank, 1 << 20)
+    start = 1 + first
     d_out = torch.empty(count, dtype=torch.int32, device="cuda")
-    cfg = hrm.make_config(args.program, variant=pick_variant(args, hrm))
+    cfg = hrm.make_config(args.program, **pick_config(args))
     L = hrm.lib()
 
     def step_device():
@@ -335,13 +346,14 @@ def run_batched(args):
     from harmonize_b200 import jobs
     specs = jobs.make_mix_specs(args.jobs, seed=1)
     mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1, sets=3)
-    variant = args.variant if args.variant >= 0 else 1
+    tc = pick_config(args, "batched", "async")
+    variant = tc["variant"]
     warm = list(range(min(48, args.jobs)))
-    jobs.batch_run(mix, 0, warm, variant=variant)
+    jobs.batch_run(mix, 0, warm, **tc)
     jobs.plain_run(mix, 1, warm)
     jobs.runtime_run(mix, 2, warm)
     with ClockSampler(0) as clk:
-        done_b, res = jobs.batch_run(mix, 0, variant=variant)
+        done_b, res = jobs.batch_run(mix, 0, **tc)
         torch.cuda.synchronize()
         done_p, plain_ms = jobs.plain_run(mix, 1, streams=16)
         torch.cuda.synchronize()
@@ -357,7 +369,7 @@ def run_batched(args):
         "steps": 1, "warmup": 1, "ms_per_step": round(span_b, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+u64", "data": "synthetic",
         "config": {"workload": f"batched_{args.jobs}_mixed_instances", "jobs": mix.total_work(),
-                   "variant": {"id": variant, "ring_links_teams_per_cta": list(hrm.VARIANTS[variant])},
+                   "variant": dict(tc, ring_links_teams_per_cta=list(hrm.VARIANTS[variant])),
                    "persistent": "one launch (CUDA graph) of AsyncProgram<MixSpec>",
                    "runtime_per_job": "one whole single-spec AsyncProgram run per job (init, exec until "
                                       "complete, synchronised), tuned variant per kind",
@@ -379,26 +391,32 @@ def run_batched(args):
 
 def run_serving(args):
     """Serving: Poisson arrivals of the job mix, rate swept as fractions of the resident runtime's
-    batched throughput; resident runtime vs one plain launch per job at the same arrivals."""
+    batched throughput; the resident runtime against, at the same arrivals, plain execution of
+    the runtime (one whole single-spec run per job, one job at a time) and one plain kernel
+    launch per job (16 streams)."""
     import harmonize_b200 as hrm
     from harmonize_b200 import jobs
     n = args.serve_jobs
     specs = jobs.make_mix_specs(n, seed=2)
-    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=2)
-    variant = args.variant if args.variant >= 0 else 1
-    done_b, res = jobs.batch_run(mix, 0, variant=variant)
+    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=2, sets=3)
+    tc = pick_config(args, "batched", "async")
+    variant = tc["variant"]
+    done_b, res = jobs.batch_run(mix, 0, **tc)
     sat = n / (res["device_ms"] / 1e3)
     rows = []
     for frac in args.rates:
         rate = frac * sat
         arr = jobs.poisson_arrivals(n, rate, seed=5)
-        lat_r, span_r = jobs.serve_replay(mix, arr, mode="resident", which=0, variant=variant)
+        lat_r, span_r = jobs.serve_replay(mix, arr, mode="resident", which=0, **tc)
         lat_p, span_p = jobs.serve_replay(mix, arr, mode="plain", which=1, streams=16)
+        lat_u, span_u = jobs.serve_replay(mix, arr, mode="runtime", which=2)
         rows.append({"load": frac, "rate_jobs_per_s": round(rate, 1),
                      "resident": dict(percentiles_ms(lat_r), jobs_per_s=round(n / (span_r / 1e3), 1)),
+                     "runtime_per_job": dict(percentiles_ms(lat_u), jobs_per_s=round(n / (span_u / 1e3), 1)),
                      "plain": dict(percentiles_ms(lat_p), jobs_per_s=round(n / (span_p / 1e3), 1))})
         print(json.dumps(rows[-1]), flush=True)
-    mism = [i for i in range(n) if not np.array_equal(mix.output(0, i), mix.output(1, i))]
+    mism = [i for i in range(n) if not (np.array_equal(mix.output(0, i), mix.output(1, i)) and
+                                        np.array_equal(mix.output(0, i), mix.output(2, i)))]
     line = {"metric": "job latency p50/p99/p99.9 (ms) and job throughput", "workload": f"serving_{n}_jobs",
             "saturation_jobs_per_s": round(sat, 1), "rates": rows,
             "outputs": "identical per job" if not mism else f"{len(mism)} jobs differ"}
@@ -406,12 +424,17 @@ def run_serving(args):
     return line
 
 
-def pick_variant(args, hrm):
-    """--variant, else the autotuner's choice for this workload and program type."""
+def pick_config(args, workload=None, program=None):
+    """--variant (with default tunables), else the autotuner's choice (variant, patience,
+    fill_links) for this workload and program type."""
     if args.variant >= 0:
-        return args.variant
-    from harmonize_b200.autotune import tuned_variant
-    return tuned_variant(args.workload, args.program)
+        return {"variant": args.variant, "patience": 0, "fill_links": 0}
+    from harmonize_b200.autotune import tuned_config
+    return tuned_config(workload or args.workload, program or args.program)
+
+
+def pick_variant(args, hrm):
+    return pick_config(args)["variant"]
 
 
 def algorithmic_bytes(stats, per_call):
@@ -505,8 +528,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
             "data": "synthetic",
             "config": dict(wl["config"], parallelism=f"replicas x{world}",
-                           variant={"id": pick_variant(args, hrm), "ring_links_teams_per_cta":
-                                    list(hrm.VARIANTS[pick_variant(args, hrm)])}),
+                           variant=dict(pick_config(args), ring_links_teams_per_cta=list(
+                               hrm.VARIANTS[pick_variant(args, hrm)]))),
             "e2e": {"value": round(e2e_value, 1), "unit": "calls/s", "h2d_bytes_per_step": wl["h2d"],
                     "d2h_bytes_per_step": wl["d2h"]},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),

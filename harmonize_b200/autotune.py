@@ -1,22 +1,30 @@
-"""Autotuner: picks the compiled tuning variant (shared-memory ring size x teams per CTA)
-with the highest async calls/s per built-in spec and program type, on the GPU it runs on.
+"""Autotuner: picks, per built-in workload and program type, the compiled variant (queue
+width = shared-memory ring links per function, and teams per CTA) and the run-time
+tunables of AsyncProgram (coalescing threshold `patience`, promise batch `fill_links` = links
+one fill takes from the arena) with the highest throughput on the GPU it runs on.
 
-    python -m harmonize_b200.autotune [--specs photon,bfs,collatz] [--reps 2]
+    python -m harmonize_b200.autotune [--specs photon,bfs,collatz,batched] [--reps 2]
 
-Writes harmonize_b200/tuned.json: {"<spec>/<program>": {"variant": v, "ring_links": r,
-"teams_per_cta": t, "calls_per_s": x, "sweep": {...}}}. bench.py and the Python wrappers
-read it; a missing entry means variant 0.
+Single-spec workloads are scored by async calls/s; "batched" (a seeded 384-job mix of all
+three specs in one persistent launch, the job-multiplexing spec) by jobs/s.
+
+Writes harmonize_b200/tuned.json: {"<workload>/<program>": {"variant": v, "ring_links": r,
+"teams_per_cta": t, "patience": p, "fill_links": f, "score": x, "unit": ..., "sweep": [...]}}.
+bench.py and the Python wrappers read it; a missing entry means variant 0 and the defaults.
+The arena size is not swept: runs size it for their work (default_arena in the C ABI).
 """
 import argparse
+import itertools
 import json
 import os
 import time
 
-import numpy as np
-
 from . import HERE, VARIANTS, bfs, collatz, photon_medium, photon_walk, rmat_csr
 
 TUNED_PATH = os.path.join(HERE, "tuned.json")
+PATIENCE = (8, 16, 64)
+FILL_LINKS = (2, 4)
+BATCH_VARIANTS = (0, 1, 2)  # the variants the job-multiplexing spec is built for
 
 
 def load_tuned():
@@ -27,56 +35,98 @@ def load_tuned():
         return {}
 
 
+def tuned_config(workload, program="async"):
+    """{variant, patience, fill_links} chosen for a workload (zeros = defaults)."""
+    e = load_tuned().get(f"{workload}/{program}", {})
+    return {"variant": int(e.get("variant", 0)), "patience": int(e.get("patience", 0)),
+            "fill_links": int(e.get("fill_links", 0))}
+
+
 def tuned_variant(spec, program):
-    return int(load_tuned().get(f"{spec}/{program}", {}).get("variant", 0))
+    return tuned_config(spec, program)["variant"]
 
 
-def _workloads():
+def _single_spec_workloads():
     mu, ab, sp = photon_medium(128, 2024)
     rp, col = rmat_csr(18, 16, 0.57, 0.19, 0.19, 1)
     return {
-        "photon": lambda prog, v: photon_walk(mu, ab, sp, 128, 0x5EED, 0, 1_000_000, program=prog, variant=v)[1],
-        "bfs": lambda prog, v: bfs(rp, col, 0, program=prog, variant=v)[1],
-        "collatz": lambda prog, v: collatz(1, 1 << 20, program=prog, variant=v)[1],
+        "photon": lambda prog, **kw: photon_walk(mu, ab, sp, 128, 0x5EED, 0, 1_000_000, program=prog, **kw)[1],
+        "bfs": lambda prog, **kw: bfs(rp, col, 0, program=prog, **kw)[1],
+        "collatz": lambda prog, **kw: collatz(1, 1 << 20, program=prog, **kw)[1],
     }
+
+
+def _candidates(prog, variants):
+    if prog == "event":  # EventProgram has no rings and no arena fills: teams per CTA only
+        return [dict(variant=v) for v in variants if v not in (1, 3)]
+    return [dict(variant=v, patience=p, fill_links=f) for v, p, f in itertools.product(variants, PATIENCE, FILL_LINKS)]
+
+
+def _best(sweep):
+    ok = [s for s in sweep if "score" in s]
+    return max(ok, key=lambda s: s["score"]) if ok else None
+
+
+def _record(table, key, best, sweep, unit):
+    v = best["variant"]
+    table[key] = {"variant": v, "ring_links": VARIANTS[v][0], "teams_per_cta": VARIANTS[v][1],
+                  "patience": best.get("patience", 0), "fill_links": best.get("fill_links", 0),
+                  "score": best["score"], "unit": unit, "sweep": sweep,
+                  "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
+    print(key, "->", json.dumps({k: table[key][k] for k in ("variant", "patience", "fill_links", "score")}),
+          flush=True)
 
 
 def tune(specs, reps=2, programs=("async", "event")):
     table = load_tuned()
-    work = _workloads()
+    work = _single_spec_workloads() if set(specs) - {"batched"} else {}
     for spec in specs:
+        if spec == "batched":
+            tune_batched(table, reps)
+            continue
         for prog in programs:
-            sweep = {}
-            for v, (ring, teams) in VARIANTS.items():
-                if prog == "event" and v in (1, 3):
-                    continue  # same event instantiation as variants 0 and 2
+            sweep = []
+            for cand in _candidates(prog, VARIANTS):
                 best = 0.0
                 try:
                     for _ in range(reps + 1):
-                        res = work[spec](prog, v)
-                        rate = res["evals"] / (res["device_ms"] / 1e3)
-                        best = max(best, rate)
-                except Exception as e:  # a variant that fails is not selectable
-                    sweep[str(v)] = {"error": str(e)}
+                        res = work[spec](prog, **cand)
+                        best = max(best, res["evals"] / (res["device_ms"] / 1e3))
+                except Exception as e:  # a configuration that fails is not selectable
+                    sweep.append(dict(cand, error=str(e)))
                     continue
-                sweep[str(v)] = {"ring_links": ring, "teams_per_cta": teams, "calls_per_s": best}
-            ok = {k: s for k, s in sweep.items() if "calls_per_s" in s}
-            if not ok:
-                continue
-            v = max(ok, key=lambda k: ok[k]["calls_per_s"])
-            table[f"{spec}/{prog}"] = {"variant": int(v), "ring_links": ok[v]["ring_links"],
-                                       "teams_per_cta": ok[v]["teams_per_cta"],
-                                       "calls_per_s": ok[v]["calls_per_s"], "sweep": sweep,
-                                       "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
-            print(spec, prog, "->", table[f"{spec}/{prog}"]["variant"], json.dumps(sweep), flush=True)
+                sweep.append(dict(cand, score=best))
+            b = _best(sweep)
+            if b:
+                _record(table, f"{spec}/{prog}", b, sweep, "calls/s")
     with open(TUNED_PATH, "w") as f:
         json.dump(table, f, indent=1, sort_keys=True)
     return table
 
 
+def tune_batched(table, reps):
+    from . import jobs
+    n = 384
+    mix = jobs.Mix(jobs.make_mix_specs(n, seed=1), photon_grid=32, media=8, seed=1)
+    sweep = []
+    for cand in _candidates("async", BATCH_VARIANTS):
+        best = 0.0
+        try:
+            for _ in range(reps + 1):
+                _, res = jobs.batch_run(mix, 0, **cand)
+                best = max(best, n / (res["device_ms"] / 1e3))
+        except Exception as e:
+            sweep.append(dict(cand, error=str(e)))
+            continue
+        sweep.append(dict(cand, score=best))
+    b = _best(sweep)
+    if b:
+        _record(table, "batched/async", b, sweep, "jobs/s")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--specs", default="photon,bfs,collatz")
+    ap.add_argument("--specs", default="photon,bfs,collatz,batched")
     ap.add_argument("--reps", type=int, default=2)
     a = ap.parse_args()
     tune(a.specs.split(","), a.reps)

@@ -754,6 +754,33 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
     }
 }
 
+int hrm_serve_replay_runtime(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int program_type,
+                             const int* variants, uint64_t* latency_ns, float* makespan_ms) {
+    if ((jobs == nullptr || arrival_ns == nullptr || latency_ns == nullptr) && njobs)
+        return hrm_capi::set_error(HRM_EINVAL, "bad replay arguments");
+    using clk = std::chrono::steady_clock;
+    try {
+        for (uint32_t j = 0; j < njobs; j++) validate(jobs[j]);
+        ck(cudaDeviceSynchronize(), "sync");
+        auto t0 = clk::now();
+        auto ns_since = [&]() {
+            return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(clk::now() - t0).count();
+        };
+        for (uint32_t j = 0; j < njobs; j++) {
+            while (ns_since() < arrival_ns[j]) std::this_thread::yield();  // FIFO: one job at a time
+            int rc = hrm_runtime_run(&jobs[j], 1, program_type, variants, nullptr, nullptr);
+            if (rc != HRM_OK) return rc;
+            latency_ns[j] = ns_since() - arrival_ns[j];
+        }
+        if (makespan_ms) *makespan_ms = (float)(ns_since() / 1e6);
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_EDEVICE, e.what());
+    }
+}
+
 int hrm_batch_run(const hrm_job* jobs, uint32_t njobs, const hrm_run_config* cfg_in, hrm_run_result* res,
                   uint64_t* done_ns) {
     if (jobs == nullptr && njobs != 0) return hrm_capi::set_error(HRM_EINVAL, "jobs is NULL");

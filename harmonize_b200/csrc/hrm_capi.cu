@@ -704,6 +704,7 @@ int collatz_run_noalloc(uint32_t start, uint32_t count, uint32_t* d_out, const h
     ctx.link_meta = (unsigned int*)(base + NA_OFF_META);
     ctx.stats = (unsigned long long*)(base + NA_OFF_STATS);
     ctx.arena_links = (unsigned int)arena;
+    NoAllocProgram::set_tunables(ctx, cfg.patience, cfg.fill_links);
     auto* it = (util::iter::AtomicIter<unsigned int>*)(base + NA_OFF_ITER);
 
     hrm_specs::CollatzState st;

@@ -12,8 +12,9 @@
 // Per job: its spec state (with a source iterator embedded in the job record), a count of
 // pending work `pending` (promises alive, plus one token per make_work in progress),
 // admission and completion timestamps (%globaltimer, ns) and a done flag. A job is done
-// when `pending` returns to zero with its source exhausted; every change of `pending` is
-// one atomicAdd per (warp, job) after __match_any_sync grouping.
+// when `pending` returns to zero with its source exhausted; changes of `pending` are
+// grouped per (warp, job) with __match_any_sync (net increments published after each
+// batch, decrements deferred: see the bookkeeping notes below).
 //
 // Serving: the host appends job records and then raises `admitted` (device memory, written
 // while the persistent kernel runs); make_work picks jobs among [0, admitted) that still
@@ -130,21 +131,22 @@ HRM_DEV HRM_FI void job_complete(const MixState& st, unsigned int j) {
 #endif
 }
 
-// Per-team bookkeeping (the mix spec's GroupState, in shared memory).
+// Pending-count bookkeeping (the mix spec's GroupState, in shared memory).
 //
-// Each evaluation records, in its lane's slot, its job and its change of that job's
-// pending count (promises created minus the one consumed). After the batch the whole team
-// settles the slots together (after_batch): lanes are grouped by job, net increments are
-// published at once and net decrements are deferred in a small table keyed by job.
+// Each evaluation records, in its lane's slot, its job and its change of that job's count
+// (promises created minus the one consumed). After the batch the whole team settles the
+// slots together (after_batch): lanes are grouped by job, net increments are published at
+// once and net decrements are deferred in a small table keyed by job.
 //
-// Why deferring decrements is safe: a job is declared complete when its published count
-// reaches zero. Increments are published before the new promises can leave the team (they
-// sit in the team's private rings until a spill, and a spill publishes with a fence), so
-// the published count never drops below the number of promises alive; holding a decrement
-// back only keeps it higher. Decrements are published, with one fence per flush instead of
-// one per batch, when an entry is evicted, every FLUSH_EVERY batches, and whenever the
-// team runs out of work (make_work, on_idle, finalize), so no completion is held back
-// while the team sleeps.
+// Why this is safe: a job is declared complete when its published count reaches zero. A
+// batch's increments are published before any promise the batch made can reach another
+// team: the new promises sit in the team's rings until the scheduler spills them (after
+// after_batch), and promises that overflow to the arena during the batch are held in the
+// team's list of unpublished links until after after_batch too. So the published count
+// never drops below the number of promises alive; holding a decrement back only keeps it
+// higher. Decrements are published, with one fence per flush instead of one per batch,
+// when an entry is evicted, every FLUSH_EVERY batches, and whenever the team runs out of
+// work (make_work, on_idle, finalize), so no completion is held back while the team sleeps.
 struct MixTeam {
     static const unsigned int SLOTS = 8;
     static const unsigned int FLUSH_EVERY = 16;
@@ -243,7 +245,7 @@ struct JobProgram {
     OUTER outer;
     STATE& device;
     unsigned int job;
-    int* delta;
+    int* delta;  // promises made by this lane for its job (settled by the team later)
 
     template <typename F, typename... A>
     HRM_DEV HRM_FI void async(A... a) {
@@ -273,10 +275,10 @@ struct Job {
         // lead to the job's buffers), and a register copy saves re-loading the job record
         // after every store the eval makes.
         S inner_state = JobStateOf<F>::get(st.jobs[job]);
-        int delta = -1;
+        int delta = -1;  // the consumed promise
         JobProgram<PROGRAM, S> jp{prog, inner_state, job, &delta};
         F::template eval<JobProgram<PROGRAM, S>>(jp, a...);
-        // Settled by the whole team after the batch (MixSpec::after_batch).
+        // Settled by the whole team after the batch (after_batch).
         MixTeam& t = prog.group;
         const unsigned int lane = util::lane_id();
         t.lane_job[lane] = job;
@@ -303,11 +305,12 @@ HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int 
     return delta;
 }
 
-// RING: ring links of the photon functions (move and collide carry a whole photon, 12
-// words; every collide batch feeds a batch of tallies, so each needs room for several
-// batches). Collatz and BFS functions get 2 links: a Collatz step makes one successor and
-// a BFS expansion overflows to the arena whatever the ring, so small rings cost them little
-// and keep a team's stash small (more resident teams per SM).
+// The functions of each job kind form one ring group (RING_GROUP_OF): a kind never calls
+// another kind's functions, so a team holds promises of one kind at a time and the three
+// kinds' rings share one stash, as large as the photon rings alone. RING: ring links of the
+// photon functions (move and collide carry a whole photon, 12 words; every collide batch
+// feeds a batch of tallies, so each needs room for several batches); the Collatz and BFS
+// functions, with 5 words or fewer, get 2*RING links in the same space.
 template <size_t RING = 4, size_t TEAMS = 4>
 struct MixSpec {
     typedef OpUnion<Job<CollatzEven>, Job<CollatzOdd>, Job<PhotonMove>, Job<PhotonCollide>, Job<PhotonTally>,
@@ -320,12 +323,15 @@ struct MixSpec {
     static const size_t RING_LINKS = 2;
     static const size_t TEAMS_PER_CTA = TEAMS;
     template <typename Op>
+    struct RING_GROUP_OF {
+        static const unsigned int value =
+            (std::is_same<Op, Job<CollatzEven>>::value || std::is_same<Op, Job<CollatzOdd>>::value) ? JOB_COLLATZ
+            : (std::is_same<Op, Job<BfsRelax>>::value || std::is_same<Op, Job<BfsExpand>>::value)  ? JOB_BFS
+                                                                                                      : JOB_PHOTON;
+    };
+    template <typename Op>
     struct RING_LINKS_OF {
-        static const size_t value = (std::is_same<Op, Job<PhotonMove>>::value ||
-                                     std::is_same<Op, Job<PhotonCollide>>::value ||
-                                     std::is_same<Op, Job<PhotonTally>>::value)
-                                        ? RING
-                                        : 2;
+        static const size_t value = RING_GROUP_OF<Op>::value == JOB_PHOTON ? RING : 2 * RING;
     };
 
     template <typename PROGRAM>
@@ -406,11 +412,11 @@ struct MixSpec {
         __syncwarp();
         delta = (int)__reduce_add_sync(0xFFFFFFFFu, (unsigned int)delta);
         if (lane == 0) {
+            // Publish the promises made and return the token (the runtime publishes the
+            // promises that overflowed to the arena only after make_work returns).
             JobRecord& r = st.jobs[j];
             if (r.source.done() && atomicCAS(&r.source_closed, 0u, 1u) == 0u) atomicAdd(st.closed, 1u);
-            __threadfence();
-            int old = atomicAdd(&r.pending, delta - 1);
-            if (old + delta - 1 == 0 && r.source.done()) job_complete(st, j);
+            job_publish(st, j, delta - 1);
         }
         return true;
 #else

@@ -33,6 +33,9 @@ def _bind():
         L.hrm_batch_run.restype = ctypes.c_int
         L.hrm_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p]
+        L.hrm_serve_replay_runtime.restype = ctypes.c_int
+        L.hrm_serve_replay_runtime.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
         L.hrm_runtime_run.restype = ctypes.c_int
         L.hrm_runtime_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
@@ -87,13 +90,20 @@ class Server:
 
 
 def serve_replay(mix, arrivals_ns, mode="resident", which=0, indices=None, streams=16, **cfg_kw):
-    """Replays arrival times against the resident runtime ("resident") or one plain launch per
-    job ("plain"). Returns (latency_ns array, makespan ms)."""
+    """Replays arrival times against the resident runtime ("resident"), one plain kernel launch
+    per job ("plain"), or one whole single-spec runtime run per job, one job at a time
+    ("runtime"). Returns (latency_ns array, makespan ms)."""
     L = _bind()
     arr = mix.job_array(which, indices)
     arrivals = np.ascontiguousarray(arrivals_ns, dtype=np.uint64)
     lat = np.zeros(len(arr), dtype=np.uint64)
     span = ctypes.c_float()
+    if mode == "runtime":
+        from .autotune import tuned_variant
+        v = (ctypes.c_int * 3)(*[tuned_variant(w, "async") for w in ("collatz", "photon", "bfs")])
+        check(L.hrm_serve_replay_runtime(ctypes.byref(arr), len(arr), arrivals.ctypes.data, 0, v, lat.ctypes.data,
+                                         ctypes.byref(span)))
+        return lat, span.value
     cfg = make_config("async", **cfg_kw)
     check(L.hrm_serve_replay(ctypes.byref(arr), len(arr), arrivals.ctypes.data, 0 if mode == "resident" else 1,
                              streams, ctypes.byref(cfg), lat.ctypes.data, ctypes.byref(span)))

@@ -99,21 +99,57 @@ class AsyncProgram {
 
     // Ring geometry: function F's ring holds ring_slots<F>() promises (RING_LINKS, or the
     // spec's RING_LINKS_OF<Op>, links of 32), and word i of its slot s is stored at
-    // words[ring_base<F>() + i * ring_slots<F>() + s] of the team's stash.
+    // words[ring_base<F>() + i * ring_slots<F>() + s] of the team's stash. Functions of
+    // different ring groups (RING_GROUP_OF) overlay one another: each group's rings start at
+    // word 0, and the stash is as large as the largest group.
     template <unsigned int F>
     __host__ __device__ static constexpr unsigned int ring_slots() {
         using Op = typename OpAt<F, OpSet>::type;
         return (unsigned int)hrm_rt::fn_RING_LINKS<PROGRAM_SPEC, Op>::value * 32u;
     }
     template <unsigned int F>
-    __host__ __device__ static constexpr unsigned int ring_base() {
+    __host__ __device__ static constexpr unsigned int group_of() {
+        using Op = typename OpAt<F, OpSet>::type;
+        return hrm_rt::fn_RING_GROUP<PROGRAM_SPEC, Op>::value;
+    }
+    template <unsigned int F>
+    __host__ __device__ static constexpr unsigned int ring_words() {
+        using Op = typename OpAt<F, OpSet>::type;
+        return Promise<Op>::WORDS * ring_slots<F>();
+    }
+    // Words used by the functions of group G before function F.
+    template <unsigned int G, unsigned int F>
+    __host__ __device__ static constexpr unsigned int group_words_before() {
         if constexpr (F == 0) {
             return 0u;
         } else {
-            using Op = typename OpAt<F - 1, OpSet>::type;
-            return ring_base<F - 1>() + Promise<Op>::WORDS * ring_slots<F - 1>();
+            return group_words_before<G, F - 1>() + (group_of<F - 1>() == G ? ring_words<F - 1>() : 0u);
         }
     }
+    template <unsigned int F>
+    __host__ __device__ static constexpr unsigned int ring_base() {
+        return group_words_before<group_of<F>(), F>();
+    }
+    template <unsigned int I>
+    __host__ __device__ static constexpr unsigned int max_group() {
+        if constexpr (I < FN) {
+            return group_of<I>() > max_group<I + 1>() ? group_of<I>() : max_group<I + 1>();
+        } else {
+            return 0u;
+        }
+    }
+    static const unsigned int RING_GROUPS = max_group<0>() + 1u;
+    template <unsigned int G>
+    __host__ __device__ static constexpr unsigned int max_group_words() {
+        if constexpr (G < RING_GROUPS) {
+            constexpr unsigned int w = group_words_before<G, FN>();
+            constexpr unsigned int rest = max_group_words<G + 1>();
+            return w > rest ? w : rest;
+        } else {
+            return 0u;
+        }
+    }
+    static const unsigned int NO_GROUP = 0xFFFFFFFFu;
     template <unsigned int I>
     __host__ __device__ static constexpr bool rings_valid() {
         if constexpr (I < FN) {
@@ -124,14 +160,22 @@ class AsyncProgram {
         }
     }
     static_assert(rings_valid<0>(), "ring sizes must be powers of two of at least 2 links");
-    static const unsigned int RING_WORDS = ring_base<FN>();
-    // Ring size of function f (run-time f).
+    static const unsigned int RING_WORDS = max_group_words<0>();
+    // Ring size and ring group of function f (run-time f).
     template <unsigned int I = 0>
     __device__ static __forceinline__ unsigned int ring_slots_of(unsigned int f) {
         if constexpr (I < FN) {
             return f == I ? ring_slots<I>() : ring_slots_of<I + 1>(f);
         } else {
             return 0u;
+        }
+    }
+    template <unsigned int I = 0>
+    __device__ static __forceinline__ unsigned int group_of_fn(unsigned int f) {
+        if constexpr (I < FN) {
+            return f == I ? group_of<I>() : group_of_fn<I + 1>(f);
+        } else {
+            return NO_GROUP;
         }
     }
 
@@ -144,9 +188,19 @@ class AsyncProgram {
     };
 
     // One team's shared-memory stash: one ring of promise slots per function.
+    // Arena links written by pushes that did not fit in the stash during one scheduling step
+    // are published when the step ends (after the batch's after_batch hook, after make_work):
+    // a spec that settles per batch (after_batch) sees its bookkeeping done before any
+    // promise of the batch can reach another team. Beyond HELD_MAX a link is published at once.
+    static const unsigned int HELD_MAX = 32;
+
     struct GroupContext {
         unsigned int count[FN];    // promises held per function (may exceed the ring briefly)
         unsigned int bottom[FN];   // ring index of the oldest promise per function
+        unsigned int active;       // ring group whose promises the stash holds, or NO_GROUP
+        unsigned int held_n;       // overflow links written and not yet published
+        unsigned int held_e[HELD_MAX];  // their queue entries
+        unsigned int held_f[HELD_MAX];  // their functions
         unsigned int words[RING_WORDS];
     };
 
@@ -161,6 +215,13 @@ class AsyncProgram {
         unsigned int patience;        // coalescing threshold in force (COALESCE_PATIENCE by default)
         unsigned int fill_links;      // links one fill may take from a queue (2 by default)
     };
+
+    // Sets a context's run-time tunables (0 = the spec's defaults; both end up >= 1). Every
+    // DeviceContext passed to a launch must go through here.
+    __host__ static void set_tunables(DeviceContext& c, unsigned int patience, unsigned int fill_links) {
+        c.patience = patience ? patience : (COALESCE_PATIENCE ? COALESCE_PATIENCE : 1u);
+        c.fill_links = fill_links ? (fill_links < 32u ? fill_links : 32u) : 2u;
+    }
 
     // -----------------------------------------------------------------------------------
     // Host-side instance: owns the device memory of one program instance.
@@ -207,8 +268,7 @@ class AsyncProgram {
             c.link_meta = link_meta.data();
             c.stats = stats.data();
             c.arena_links = (unsigned int)arena_size;
-            c.patience = patience ? patience : COALESCE_PATIENCE;
-            c.fill_links = fill_links ? (fill_links < 32u ? fill_links : 32u) : 2u;
+            set_tunables(c, patience, fill_links);
             return c;
         }
 
@@ -375,6 +435,24 @@ class AsyncProgram {
         const unsigned int rank = __popc(mask & util::lanemask_lt());
         const unsigned int leader = __ffs(mask) - 1;
         GroupContext& g = _grp_ctx;
+        if constexpr (RING_GROUPS > 1) {
+            // The stash holds one ring group at a time: claim it if empty; a promise of
+            // another group goes to the arena, where a team of that group will take it.
+            constexpr unsigned int G = group_of<F>();
+            unsigned int mine = 1u;
+            if (rank == 0) {
+                unsigned int a = *(volatile unsigned int*)&g.active;
+                if (a == NO_GROUP) a = atomicCAS(&g.active, NO_GROUP, G);
+                mine = (a == NO_GROUP || a == G) ? 1u : 0u;
+            }
+            if (__shfl_sync(mask, mine, leader) == 0u) {
+                unsigned int spill_w[W];  // the out-of-line path takes a copy (see below)
+#pragma unroll
+                for (unsigned int i = 0; i < W; i++) spill_w[i] = w[i];
+                overflow_to_arena<TYPE>(spill_w, mask);
+                return;
+            }
+        }
         unsigned int base = 0;
         if (rank == 0) base = atomicAdd(&g.count[F], (unsigned int)__popc(mask));
         base = __shfl_sync(mask, base, leader);
@@ -386,15 +464,20 @@ class AsyncProgram {
             for (unsigned int i = 0; i < W; i++) g.words[BASE + i * SLOTS + slot] = w[i];
         }
         if (over != 0 && idx >= SLOTS) {
-            overflow_to_arena<TYPE>(w, over);
+            unsigned int spill_w[W];
+#pragma unroll
+            for (unsigned int i = 0; i < W; i++) spill_w[i] = w[i];
+            overflow_to_arena<TYPE>(spill_w, over);
         }
     }
 
     // Lanes in `over` could not fit in shared memory: write them straight to one arena link
-    // and publish it to the function's queue. (Inlined so that the promise words stay in
-    // registers: a call taking them by reference would put every push's words on the stack.)
+    // and publish it to the function's queue. Out of line, so that every push site stays
+    // small (the instruction cache is the first limit of a kernel with many async functions);
+    // callers pass a copy of the words made only on this rare path, so that the words of
+    // ordinary pushes stay in registers instead of going through the stack.
     template <typename TYPE>
-    __device__ __forceinline__ void overflow_to_arena(const unsigned int (&w)[Promise<TYPE>::WORDS], unsigned int over) {
+    __device__ __noinline__ void overflow_to_arena(const unsigned int (&w)[Promise<TYPE>::WORDS], unsigned int over) {
         constexpr unsigned int F = disc_of<TYPE>();
         constexpr unsigned int W = Promise<TYPE>::WORDS;
         const unsigned int r = __popc(over & util::lanemask_lt());
@@ -411,7 +494,32 @@ class AsyncProgram {
         for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, r), w[i]);
         __threadfence();
         __syncwarp(over);
-        hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, n), r, 1, over);
+        if (r == 0) {
+            const unsigned int e = hrm_rt::encode_link(link, n);
+            const unsigned int slot = atomicAdd(&_grp_ctx.held_n, 1u);
+            if (slot < HELD_MAX) {
+                _grp_ctx.held_e[slot] = e;
+                _grp_ctx.held_f[slot] = F;
+            } else {
+                hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, e, 0, 1, 1u << util::lane_id());
+            }
+        }
+        __syncwarp(over);
+    }
+
+    // Whole team: publishes the overflow links held during this step.
+    __device__ __forceinline__ void publish_held() {
+        __syncwarp();
+        const unsigned int n = min(_grp_ctx.held_n, HELD_MAX);
+        if (n == 0) return;
+        const unsigned int lane = util::lane_id();
+        if (lane < n) {
+            hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, _grp_ctx.held_f[lane], _grp_ctx.held_e[lane], 0, 1,
+                              1u << lane);
+        }
+        __syncwarp();
+        if (lane == 0) _grp_ctx.held_n = 0;
+        __syncwarp();
     }
 
     // -----------------------------------------------------------------------------------
@@ -476,9 +584,10 @@ class AsyncProgram {
     // Scheduler (whole team converged).
     // ===================================================================================
 
-    // Moves the oldest min(count, nlinks*32) promises of function f to the arena.
+    // Moves the oldest min(count, nlinks*32) promises of function f to the arena; returns the
+    // links written. Out of line: it is reached from several places of the scheduler.
     template <unsigned int F>
-    __device__ void spill_typed(unsigned int nlinks, unsigned long long& spilled) {
+    __device__ __noinline__ unsigned int spill_typed(unsigned int nlinks) {
         using Op = typename OpAt<F, OpSet>::type;
         constexpr unsigned int W = Promise<Op>::WORDS;
         constexpr unsigned int SLOTS = ring_slots<F>();
@@ -487,14 +596,14 @@ class AsyncProgram {
         const unsigned int lane = util::lane_id();
         unsigned int cnt = g.count[F];
         unsigned int n = min(cnt, nlinks * 32u);
-        if (n == 0) return;
+        if (n == 0) return 0u;
         unsigned int nl = (n + 31u) / 32u;
         unsigned int link = 0xFFFFFFFFu;
         unsigned int got = alloc_links_coop(nl, lane, 0xFFFFFFFFu, link);
         if (got < nl) {
             // Return what we obtained and keep the promises in shared memory.
             if (got > 0) free_links_coop(link, lane, got, 0xFFFFFFFFu);
-            return;
+            return 0u;
         }
         const unsigned int bottom = g.bottom[F];
         for (unsigned int l = 0; l < nl; l++) {
@@ -516,13 +625,13 @@ class AsyncProgram {
             g.count[F] = cnt - n;
         }
         __syncwarp();
-        spilled += nl;
+        return nl;
     }
 
     template <unsigned int I>
-    __device__ void spill_fn(unsigned int f, unsigned int nlinks, unsigned long long& spilled) {
+    __device__ __forceinline__ void spill_fn(unsigned int f, unsigned int nlinks, unsigned long long& spilled) {
         if constexpr (I < FN) {
-            if (f == I) spill_typed<I>(nlinks, spilled);
+            if (f == I) spilled += spill_typed<I>(nlinks);
             else spill_fn<I + 1>(f, nlinks, spilled);
         }
     }
@@ -668,6 +777,10 @@ class AsyncProgram {
             _grp_ctx.count[lane] = 0;
             _grp_ctx.bottom[lane] = 0;
         }
+        if (lane == 0) {
+            _grp_ctx.active = NO_GROUP;
+            _grp_ctx.held_n = 0;
+        }
         __syncwarp();
     }
 
@@ -679,6 +792,7 @@ class AsyncProgram {
         init_team();
         hrm_rt::call_initialize<PROGRAM_SPEC>(*this);
         __syncwarp();
+        publish_held();
 
         GroupContext& g = _grp_ctx;
         hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
@@ -692,6 +806,7 @@ class AsyncProgram {
         unsigned int rotate = 0;          // next function to favour for a forced partial batch
         bool quiescent = false;
         const unsigned int my_ring = (lane < FN) ? ring_slots_of(lane) : 0u;  // lane f: f's ring size
+        const unsigned int my_group = (lane < FN) ? group_of_fn(lane) : NO_GROUP;  // lane f: f's ring group
 
         for (unsigned int cycle = 0; cycle < cycle_count; cycle++) {
             // Stop on a halt request or an error flag.
@@ -702,10 +817,22 @@ class AsyncProgram {
                 if (fl & (EARLY_HALT_FLAG | hrm_rt::ERROR_MASK)) break;
             }
 
-            // Pick the fullest function.
+            // Pick the fullest function, except that a function past its high-water mark
+            // (fewer than 32 free slots) runs first: it always holds a full batch (rings have
+            // at least 64 slots), and running it makes the room that running another
+            // function would otherwise have to make by spilling it to the arena.
             unsigned int c = (lane < FN) ? g.count[lane] : 0u;
+            if constexpr (RING_GROUPS > 1) {
+                // An empty stash belongs to no ring group.
+                if (__all_sync(0xFFFFFFFFu, lane >= FN || c == 0u) && lane == 0) g.active = NO_GROUP;
+                __syncwarp();
+            }
             unsigned int key = (lane < FN) ? ((min(c, 0xFFFFu) << 5) | lane) : 0u;
-            unsigned int best = __reduce_max_sync(0xFFFFFFFFu, key);
+            const unsigned int over = (lane < FN && c > my_ring - 32u) ? c - (my_ring - 32u) : 0u;
+            const unsigned int okey = over ? ((min(over, 0xFFFFu) << 5) | lane) : 0u;
+            const unsigned int obest = __reduce_max_sync(0xFFFFFFFFu, okey);
+            unsigned int best = obest ? ((min(__shfl_sync(0xFFFFFFFFu, c, obest & 31u), 0xFFFFu) << 5) | (obest & 31u))
+                                      : __reduce_max_sync(0xFFFFFFFFu, key);
             unsigned int bf = best & 31u, bc = best >> 5;
 
             // A partial batch that stops growing is starving: other work (full batches of
@@ -732,13 +859,33 @@ class AsyncProgram {
                 // No full batch locally: try the arena for the function closest to full.
                 unsigned int av = 0;
                 if (lane < FN) av = hrm_rt::ld_relaxed(&_dev_ctx.rings.heads[lane].avail);
-                unsigned int fkey = (lane < FN && (int)av > 0) ? (((min(c, 0xFFFFu) + 1u) << 5) | lane) : 0u;
+                // With ring groups, only the active group's queues (any, if the stash is empty).
+                const unsigned int act = (RING_GROUPS > 1) ? g.active : 0u;
+                const bool own = lane < FN && (RING_GROUPS == 1 || act == NO_GROUP || my_group == act);
+                unsigned int fkey = (own && (int)av > 0) ? (((min(c, 0xFFFFu) + 1u) << 5) | lane) : 0u;
                 unsigned int fbest = __reduce_max_sync(0xFFFFFFFFu, fkey);
+                if constexpr (RING_GROUPS > 1) {
+                    // Work of another group waits in the arena and this team has no full batch
+                    // nor queued work of its own: hand its partial work to the arena and change
+                    // group, instead of making more work of its own group.
+                    if (fbest == 0 && act != NO_GROUP &&
+                        __any_sync(0xFFFFFFFFu, lane < FN && my_group != act && (int)av > 0)) {
+                        for (unsigned int f = 0; f < FN; f++) {
+                            unsigned int cf = g.count[f];
+                            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
+                        }
+                        if (__all_sync(0xFFFFFFFFu, lane >= FN || g.count[lane] == 0u)) continue;
+                    }
+                }
                 if (fbest != 0) {
                     unsigned int ff = fbest & 31u;
                     if (counted_idle) {
                         if (lane == 0) atomicAdd(&ctl->busy_epoch, hrm_rt::BUSY_ONE + 1ull);
                         counted_idle = false;
+                    }
+                    if constexpr (RING_GROUPS > 1) {
+                        if (act == NO_GROUP && lane == 0) g.active = group_of_fn(ff);
+                        __syncwarp();
                     }
                     unsigned int took = fill_fn<0>(ff);
                     n_fill += took;
@@ -756,6 +903,7 @@ class AsyncProgram {
                     }
                     const unsigned int before = __reduce_add_sync(0xFFFFFFFFu, c);
                     bool more = hrm_rt::call_make_work<PROGRAM_SPEC>(*this);
+                    publish_held();
                     can_make_work = __any_sync(0xFFFFFFFFu, more);
                     n_mw++;
                     clamp_counts();
@@ -798,6 +946,7 @@ class AsyncProgram {
             }
             run_fn<0>(bf, k);
             hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
+            publish_held();
             clamp_counts();
             n_evals += k;
             n_batches += 1;
@@ -807,6 +956,7 @@ class AsyncProgram {
 
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
         __syncwarp();
+        publish_held();
 
         // Leave nothing in shared memory: spill every pending promise.
         for (unsigned int f = 0; f < FN; f++) {

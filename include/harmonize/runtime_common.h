@@ -66,6 +66,18 @@ template <class S, class Op>
 struct fn_RING_LINKS<S, Op, std::void_t<decltype(S::template RING_LINKS_OF<Op>::value)>>
     : std::integral_constant<size_t, (size_t)(S::template RING_LINKS_OF<Op>::value)> {};
 
+// Ring groups: a spec whose functions fall into groups that never call one another (for
+// example the functions of independent programs multiplexed in one launch) may define
+//   template <typename Op> struct RING_GROUP_OF { static const unsigned int value = ...; };
+// The rings of different groups then share the same shared memory: a team holds promises of
+// one group at a time and changes group only when its rings are empty. A push of another
+// group's promise goes to the arena. Default: one group.
+template <class S, class Op, class = void>
+struct fn_RING_GROUP : std::integral_constant<unsigned int, 0u> {};
+template <class S, class Op>
+struct fn_RING_GROUP<S, Op, std::void_t<decltype(S::template RING_GROUP_OF<Op>::value)>>
+    : std::integral_constant<unsigned int, (unsigned int)(S::template RING_GROUP_OF<Op>::value)> {};
+
 template <class S, class P, class = void>
 struct has_initialize : std::false_type {};
 template <class S, class P>

@@ -265,6 +265,11 @@ int hrm_server_destroy(hrm_server* srv);
  * latency_ns[j] = host-observed completion minus arrival; *makespan_ms = time to the last. */
 int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int mode, uint32_t nstreams,
                      const hrm_run_config* cfg, uint64_t* latency_ns, float* makespan_ms);
+/* The same replay against plain execution of the runtime itself: jobs served one at a time in
+ * arrival order, each by one whole single-spec run (as hrm_runtime_run; variants per job kind,
+ * NULL = 0). */
+int hrm_serve_replay_runtime(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int program_type,
+                             const int* variants, uint64_t* latency_ns, float* makespan_ms);
 
 /* ---- run without device allocation ------------------------------------------------------
  * No counterpart in the original Harmonize (every original program instance allocates its
