@@ -13,8 +13,8 @@
 // pending work `pending` (promises alive, plus one token per make_work in progress),
 // admission and completion timestamps (%globaltimer, ns) and a done flag. A job is done
 // when `pending` returns to zero with its source exhausted; changes of `pending` are
-// grouped per (warp, job) with __match_any_sync (net increments published after each
-// batch, decrements deferred: see the bookkeeping notes below).
+// grouped per (warp, job) with __match_any_sync and collected in a per-team table that is
+// published in batches (see the bookkeeping notes below).
 //
 // Serving: the host appends job records and then raises `admitted` (device memory, written
 // while the persistent kernel runs); make_work picks jobs among [0, admitted) that still
@@ -135,21 +135,24 @@ HRM_DEV HRM_FI void job_complete(const MixState& st, unsigned int j) {
 //
 // Each evaluation records, in its lane's slot, its job and its change of that job's count
 // (promises created minus the one consumed). After the batch the whole team settles the
-// slots together (after_batch): lanes are grouped by job, net increments are published at
-// once and net decrements are deferred in a small table keyed by job.
+// slots together (after_batch): lanes are grouped by job and each group's net change is
+// added to a small per-team table keyed by job. Increases in the table are published
+// (relaxed atomics) before any promise of the team becomes visible to other teams
+// (before_publish: spills, overflow links held during a step) and when evicted; decreases
+// (one fence per flush, with the completion check) when evicted, every FLUSH_EVERY batches,
+// and whenever the team runs out of work (make_work, on_idle, finalize).
 //
-// Why this is safe: a job is declared complete when its published count reaches zero. A
-// batch's increments are published before any promise the batch made can reach another
-// team: the new promises sit in the team's rings until the scheduler spills them (after
-// after_batch), and promises that overflow to the arena during the batch are held in the
-// team's list of unpublished links until after after_batch too. So the published count
-// never drops below the number of promises alive; holding a decrement back only keeps it
-// higher. Decrements are published, with one fence per flush instead of one per batch,
-// when an entry is evicted, every FLUSH_EVERY batches, and whenever the team runs out of
-// work (make_work, on_idle, finalize), so no completion is held back while the team sleeps.
+// Why this is safe. Let D_t be team t's unpublished net change of a job. If D_t > 0, look at
+// the last moment t published promises (or the entry's creation): D_t was <= 0 then, so
+// since then t made more promises than it consumed; those promises are all still in t's
+// rings or were consumed by t (nothing was published since), and t made them by consuming
+// older promises, so D_t is at most (the job's promises alive in t's rings) - 1. The
+// published count is (promises alive) - sum of D_t, which is therefore at least one while
+// any promise is alive and never below zero; it reaches zero only when no promise is alive
+// and nothing is held: a job is declared complete exactly when it is.
 struct MixTeam {
-    static const unsigned int SLOTS = 8;
-    static const unsigned int FLUSH_EVERY = 16;
+    static const unsigned int SLOTS = 16;
+    static const unsigned int FLUSH_EVERY = 64;
     static const unsigned int EMPTY = 0xFFFFFFFFu;
     unsigned int lane_job[32];  // job of the lane's evaluation in this batch, or EMPTY
     int lane_delta[32];
@@ -159,8 +162,8 @@ struct MixTeam {
     unsigned int used;  // bit s set while job[s] holds an entry
 };
 
-// One lane: publishes a decrement of job j, completing the job at zero with its source
-// exhausted. The fence orders this team's writes of the job's results before the count.
+// One lane: publishes a decrease of job j's count, completing the job at zero with its
+// source exhausted. The fence orders this team's writes of the job's results before the count.
 HRM_DEV HRM_FI void job_publish(const MixState& st, unsigned int j, int d) {
 #if defined(__CUDA_ARCH__)
     __threadfence();
@@ -169,27 +172,42 @@ HRM_DEV HRM_FI void job_publish(const MixState& st, unsigned int j, int d) {
 #endif
 }
 
-// One lane: publishes every deferred decrement of the team.
-HRM_DEV HRM_FI void team_flush(const MixState& st, MixTeam& t) {
+// Publishing a net increase never completes a job (the published count is never below
+// zero, so it rises from zero or more) and orders nothing: a relaxed atomic, no fence.
+HRM_DEV HRM_FI void job_raise(const MixState& st, unsigned int j, int d) {
 #if defined(__CUDA_ARCH__)
-    unsigned int used = t.used;
-    if (used != 0u) {
-        __threadfence();
-        while (used) {
-            unsigned int s = __ffs(used) - 1;
-            used &= used - 1;
-            int d = t.delta[s];
-            int old = atomicAdd(&st.jobs[t.job[s]].pending, d);
-            if (old + d == 0 && st.jobs[t.job[s]].source.done()) job_complete(st, t.job[s]);
-            t.job[s] = MixTeam::EMPTY;
-        }
-        t.used = 0u;
-    }
-    t.settles = 0u;
+    atomicAdd(&st.jobs[j].pending, d);
 #endif
 }
 
-// One lane: records a decrement of job j in the team table.
+// One lane: publishes the team table's increases (negatives = false) or every entry.
+HRM_DEV HRM_FI void team_flush(const MixState& st, MixTeam& t, bool negatives) {
+#if defined(__CUDA_ARCH__)
+    unsigned int used = t.used;
+    bool fenced = false;
+    while (used) {
+        const unsigned int s = __ffs(used) - 1;
+        used &= used - 1;
+        const int d = t.delta[s];
+        if (d < 0 && !negatives) continue;
+        if (d > 0) {
+            job_raise(st, t.job[s], d);
+        } else if (d < 0) {
+            if (!fenced) {
+                __threadfence();  // this team's writes of job results before the counts
+                fenced = true;
+            }
+            const int old = atomicAdd(&st.jobs[t.job[s]].pending, d);
+            if (old + d == 0 && st.jobs[t.job[s]].source.done()) job_complete(st, t.job[s]);
+        }
+        t.job[s] = MixTeam::EMPTY;
+        t.used &= ~(1u << s);
+    }
+    if (negatives) t.settles = 0u;
+#endif
+}
+
+// One lane: adds a change of job j's count to the team table.
 HRM_DEV HRM_FI void team_defer(const MixState& st, MixTeam& t, unsigned int j, int d) {
     const unsigned int s = j & (MixTeam::SLOTS - 1u);
     const unsigned int bit = 1u << s;
@@ -197,7 +215,11 @@ HRM_DEV HRM_FI void team_defer(const MixState& st, MixTeam& t, unsigned int j, i
         t.delta[s] += d;
         return;
     }
-    if ((t.used & bit) != 0u) job_publish(st, t.job[s], t.delta[s]);  // evict the other job
+    if ((t.used & bit) != 0u) {  // evict the other job
+        const int e = t.delta[s];
+        if (e > 0) job_raise(st, t.job[s], e);
+        else if (e < 0) job_publish(st, t.job[s], e);
+    }
     t.job[s] = j;
     t.delta[s] = d;
     t.used |= bit;
@@ -214,8 +236,7 @@ HRM_DEV HRM_FI void team_settle(const MixState& st, MixTeam& t) {
     const unsigned int grp = __match_any_sync(0xFFFFFFFFu, j);
     const int sum = (int)__reduce_add_sync(grp, (unsigned int)delta);
     const bool leader = j != MixTeam::EMPTY && lane == (unsigned int)(__ffs(grp) - 1);
-    if (leader && sum > 0) atomicAdd(&st.jobs[j].pending, sum);  // a rising count completes nothing
-    unsigned int defer = __ballot_sync(0xFFFFFFFFu, leader && sum < 0);
+    unsigned int defer = __ballot_sync(0xFFFFFFFFu, leader && sum != 0);
     // One lane at a time updates the table (it belongs to this team alone).
     while (defer) {
         const unsigned int src = __ffs(defer) - 1;
@@ -223,18 +244,18 @@ HRM_DEV HRM_FI void team_settle(const MixState& st, MixTeam& t) {
         if (lane == src) team_defer(st, t, j, sum);
         __syncwarp();
     }
-    if (lane == 0 && ++t.settles >= MixTeam::FLUSH_EVERY) team_flush(st, t);
+    if (lane == 0 && ++t.settles >= MixTeam::FLUSH_EVERY) team_flush(st, t, true);
     __syncwarp();
 #endif
 }
 
-// Whole team: publishes every deferred decrement.
-HRM_DEV HRM_FI void team_flush_all(const MixState& st, MixTeam& t) {
+// Whole team: publishes the table's increases, or (negatives) every entry.
+HRM_DEV HRM_FI void team_flush_all(const MixState& st, MixTeam& t, bool negatives = true) {
 #if defined(__CUDA_ARCH__)
     __syncwarp();
     unsigned int lane;
     asm volatile("mov.u32 %0, %%laneid;" : "=r"(lane));
-    if (lane == 0) team_flush(st, t);
+    if (lane == 0) team_flush(st, t, negatives);
     __syncwarp();
 #endif
 }
@@ -358,6 +379,10 @@ struct MixSpec {
     template <typename PROGRAM>
     HRM_DEV static void after_batch(PROGRAM prog) {
         team_settle(prog.device, prog.group);
+    }
+    template <typename PROGRAM>
+    HRM_DEV static void before_publish(PROGRAM prog) {
+        team_flush_all(prog.device, prog.group, false);  // increases only: decreases may wait
     }
 
     // Called by a whole team: picks one job that still has sources (round robin over the

@@ -233,3 +233,40 @@ def plain_run(mix, which=1, indices=None, streams=16):
     total = ctypes.c_float()
     check(L.hrm_plain_run(ctypes.byref(arr), len(arr), streams, done.ctypes.data, ctypes.byref(total)))
     return done, total.value
+
+
+def main(argv=None):
+    """Runs one batch of jobs from the command line and prints its result as JSON:
+
+        python -m harmonize_b200.jobs [--jobs N] [--seed S] [--kind collatz|photon|bfs]
+                                      [--photon-job COUNT] [--variant V] [--arena LINKS]
+
+    --photon-job COUNT runs a single photon job of COUNT photons on a 32^3 medium (the case
+    used to profile the batched kernel); otherwise the seeded job mix of N jobs, optionally
+    restricted to one kind."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--jobs", type=int, default=384)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--kind", choices=list(KIND_NAMES.values()), default=None)
+    ap.add_argument("--photon-job", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=2)
+    ap.add_argument("--arena", type=int, default=0)
+    a = ap.parse_args(argv)
+    if a.photon_job:
+        specs = [{"kind": JOB_PHOTON, "first": 0, "count": a.photon_job, "seed": 0x1234567, "medium": 0}]
+        mix = Mix(specs, photon_grid=32, media=1, seed=a.seed)
+        idx = None
+    else:
+        mix = Mix(make_mix_specs(a.jobs, seed=a.seed), photon_grid=32, media=8, seed=a.seed)
+        kinds = {v: k for k, v in KIND_NAMES.items()}
+        idx = None if a.kind is None else [i for i, s in enumerate(mix.specs) if s["kind"] == kinds[a.kind]]
+    done, res = batch_run(mix, 0, indices=idx, variant=a.variant, arena=a.arena)
+    res["jobs"] = len(done)
+    res["calls_per_s"] = res["evals"] / (res["device_ms"] / 1e3)
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

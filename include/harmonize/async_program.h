@@ -512,6 +512,8 @@ class AsyncProgram {
         __syncwarp();
         const unsigned int n = min(_grp_ctx.held_n, HELD_MAX);
         if (n == 0) return;
+        hrm_rt::call_before_publish<PROGRAM_SPEC>(*this);
+        __syncwarp();
         const unsigned int lane = util::lane_id();
         if (lane < n) {
             hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, _grp_ctx.held_f[lane], _grp_ctx.held_e[lane], 0, 1,
@@ -870,6 +872,8 @@ class AsyncProgram {
                     // group, instead of making more work of its own group.
                     if (fbest == 0 && act != NO_GROUP &&
                         __any_sync(0xFFFFFFFFu, lane < FN && my_group != act && (int)av > 0)) {
+                        hrm_rt::call_before_publish<PROGRAM_SPEC>(*this);
+                        __syncwarp();
                         for (unsigned int f = 0; f < FN; f++) {
                             unsigned int cf = g.count[f];
                             if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
@@ -937,6 +941,10 @@ class AsyncProgram {
             // Every other ring needs one link of headroom for the calls this batch makes
             // (the batch's own ring frees k slots when it is popped).
             unsigned int hi = __ballot_sync(0xFFFFFFFFu, lane < FN && lane != bf && c > my_ring - 32u);
+            if (hi) {
+                hrm_rt::call_before_publish<PROGRAM_SPEC>(*this);
+                __syncwarp();
+            }
             while (hi) {
                 unsigned int f = __ffs(hi) - 1;
                 hi &= hi - 1;
@@ -957,6 +965,8 @@ class AsyncProgram {
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
         __syncwarp();
         publish_held();
+        hrm_rt::call_before_publish<PROGRAM_SPEC>(*this);
+        __syncwarp();
 
         // Leave nothing in shared memory: spill every pending promise.
         for (unsigned int f = 0; f < FN; f++) {

@@ -128,6 +128,19 @@ template <class S, class P>
 __device__ __forceinline__ void call_on_idle(P prog) {
     if constexpr (has_on_idle<S, P>::value) S::template on_idle<P>(prog);
 }
+//   template <class P> __device__ static void before_publish(P prog);
+//     called by the whole team, converged, right before promises of the team become visible
+//     to other teams (spills, overflow links held during a step), so that bookkeeping about
+//     them can be published first.
+template <class S, class P, class = void>
+struct has_before_publish : std::false_type {};
+template <class S, class P>
+struct has_before_publish<S, P, std::void_t<decltype(S::template before_publish<P>(std::declval<P>()))>>
+    : std::true_type {};
+template <class S, class P>
+__device__ __forceinline__ void call_before_publish(P prog) {
+    if constexpr (has_before_publish<S, P>::value) S::template before_publish<P>(prog);
+}
 template <class S, class P, class = void>
 struct has_after_batch : std::false_type {};
 template <class S, class P>
