@@ -181,6 +181,11 @@ def flush_l2(buf):
 #   BFS Expand     : 2 x 12 B promise + 8 B rowptr + 4 B per edge read (counted on Relax side: 4 B)
 #   Collatz Even/Odd: 2 x 16 B promise (+ 4 B output once per start, ignored) = 32 B
 # ---------------------------------------------------------------------------------------
+# Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one exec launch on a
+# small case of the same kernel, with its call count: scaled by calls to the bench's launch
+# (profiles/photon_walk_async_exec_kernel_ncu.txt: 10^5 photons, variant R4/T2).
+TRAFFIC_PROFILE = {("photon", "async"): (2792448 + 1518080, 161486336)}
+
 BYTES_PER_CALL = {
     "photon": [93, 92, 48],
     "bfs": [24 + 4, 24 + 8],
@@ -508,8 +513,11 @@ def main():
     s0 = stats_all[-1]
     alg = algorithmic_bytes(s0, wl["bytes_per_call"])
     achieved_gbs = alg / (step_ms[-1] / 1e3) / 1e9
+    prof = TRAFFIC_PROFILE.get((args.workload, args.program))
+    traffic = round(prof[0] / prof[1] * s0["evals"]) if prof else None
     roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": None,
+                "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": traffic,
+                "traffic_source": ("ncu DRAM bytes of a 10^5-photon launch scaled by calls" if prof else None),
                 "peak_source": pk["source"],
                 "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes = each call's promise written and read once plus its compulsory "

@@ -408,6 +408,16 @@ struct Server : ServerBase {
         ck(cudaMemcpy(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice), "counters");
         P::launch_init(inst, groups, exec_s);
         ck(cudaStreamSynchronize(exec_s), "init");
+        // Load the kernels that the session launches while its persistent kernel runs. A
+        // kernel loaded on first use (lazy module loading) cannot start until the running
+        // persistent kernel ends, which held the first jobs of a session back by one whole
+        // exec (seconds).
+        cudaFuncAttributes fa;
+        ck(cudaFuncGetAttributes(&fa, mix_prepare_range_kernel), "kernel load");
+        ck(cudaFuncGetAttributes(&fa, halt_kernel), "kernel load");
+        mix_prepare_range_kernel<<<1, 32, 0, submit_s>>>(jobs.data(), 0u, 0u);
+        ck(cudaGetLastError(), "kernel load");
+        ck(cudaStreamSynchronize(submit_s), "kernel load");
         runner = std::thread([this] { loop(); });
     }
 

@@ -230,6 +230,43 @@ struct DeviceArray {
     DeviceArray& operator=(const DeviceArray&) = delete;
 };
 
+// Device copies of the inputs and outputs of the host-buffer whole runs (hrm_*_run), kept per
+// device and grown on demand, so that repeated runs allocate nothing: allocating and freeing
+// tens of MB per call cost up to a second of host time in measurement. A host-buffer run
+// holds its device's staging lock from upload to download.
+struct Staging {
+    std::mutex lock;
+    std::vector<std::pair<void*, size_t>> bufs;  // slot -> (device pointer, bytes)
+    template <typename T>
+    T* get(size_t slot, size_t count) {
+        const size_t bytes = count * sizeof(T) ? count * sizeof(T) : 16;
+        if (bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
+        auto& b = bufs[slot];
+        if (b.second < bytes) {
+            if (b.first) ck(cudaFree(b.first), "cudaFree");
+            b = {nullptr, 0};
+            ck(cudaMalloc(&b.first, bytes), "cudaMalloc");
+            b.second = bytes;
+        }
+        return (T*)b.first;
+    }
+    ~Staging() {
+        for (auto& b : bufs)
+            if (b.first) cudaFree(b.first);
+    }
+};
+std::mutex g_staging_mutex;
+std::map<int, std::unique_ptr<Staging>> g_staging;
+
+Staging& staging() {
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(g_staging_mutex);
+    auto& s = g_staging[dev];
+    if (!s) s.reset(new Staging());
+    return *s;
+}
+
 // Program instances of the whole-run helpers, kept per (device, spec, type, variant,
 // arena) and re-initialised by every run, so that repeated runs allocate nothing.
 struct CacheKey {
@@ -420,8 +457,12 @@ int hrm_device_sync(void) {
 
 int hrm_release_cache(void) {
     HRM_GUARD({
-        std::lock_guard<std::mutex> lock(g_cache_mutex);
-        g_cache.clear();
+        {
+            std::lock_guard<std::mutex> lock(g_cache_mutex);
+            g_cache.clear();
+        }
+        std::lock_guard<std::mutex> lock(g_staging_mutex);
+        g_staging.clear();
         return HRM_OK;
     })
 }
@@ -531,10 +572,12 @@ int hrm_collatz_run(uint32_t start, uint32_t count, uint32_t* out, const hrm_run
     HRM_GUARD({
         hrm_run_config cfg = config_or_default(cfg_in);
         cudaStream_t s = (cudaStream_t)cfg.stream;
-        DeviceArray<uint32_t> d(count);
-        int rc = collatz_run(start, count, d.ptr, &cfg, res);
+        Staging& st = staging();
+        std::lock_guard<std::mutex> staged(st.lock);
+        uint32_t* d = st.get<uint32_t>(0, count);
+        int rc = collatz_run(start, count, d, &cfg, res);
         if (rc != HRM_OK) return rc;
-        ck(cudaMemcpyAsync(out, d.ptr, (size_t)count * 4u, cudaMemcpyDeviceToHost, s), "output download");
+        ck(cudaMemcpyAsync(out, d, (size_t)count * 4u, cudaMemcpyDeviceToHost, s), "output download");
         ck(cudaStreamSynchronize(s), "output download");
         return HRM_OK;
     })
@@ -557,15 +600,18 @@ int hrm_photon_run(const float* mu_s, const float* absorb, const uint8_t* split,
         cudaStream_t s = (cudaStream_t)cfg.stream;
         const size_t nvox = (size_t)n * n * n;
         const size_t slots = nvox + 3u * hrm_specs::PHOTON_SPREAD;
-        DeviceArray<float> dm(nvox), da(nvox);
-        DeviceArray<uint8_t> dsp(nvox);
-        DeviceArray<uint64_t> dt(slots);
-        ck(cudaMemcpyAsync(dm.ptr, mu_s, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
-        ck(cudaMemcpyAsync(da.ptr, absorb, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
-        ck(cudaMemcpyAsync(dsp.ptr, split, nvox, cudaMemcpyHostToDevice, s), "medium upload");
-        int rc = photon_run(dm.ptr, da.ptr, dsp.ptr, n, seed, first, count, dt.ptr, &cfg, res);
+        Staging& st = staging();
+        std::lock_guard<std::mutex> staged(st.lock);
+        float* dm = st.get<float>(0, nvox);
+        float* da = st.get<float>(1, nvox);
+        uint8_t* dsp = st.get<uint8_t>(2, nvox);
+        uint64_t* dt = st.get<uint64_t>(3, slots);
+        ck(cudaMemcpyAsync(dm, mu_s, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
+        ck(cudaMemcpyAsync(da, absorb, nvox * 4u, cudaMemcpyHostToDevice, s), "medium upload");
+        ck(cudaMemcpyAsync(dsp, split, nvox, cudaMemcpyHostToDevice, s), "medium upload");
+        int rc = photon_run(dm, da, dsp, n, seed, first, count, dt, &cfg, res);
         if (rc != HRM_OK) return rc;
-        ck(cudaMemcpyAsync(tally, dt.ptr, slots * 8u, cudaMemcpyDeviceToHost, s), "tally download");
+        ck(cudaMemcpyAsync(tally, dt, slots * 8u, cudaMemcpyDeviceToHost, s), "tally download");
         ck(cudaStreamSynchronize(s), "tally download");
         return HRM_OK;
     })
@@ -585,12 +631,16 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
         hrm_run_config cfg = config_or_default(cfg_in);
         cudaStream_t s = (cudaStream_t)cfg.stream;
         const size_t ne = rowptr[nv];
-        DeviceArray<uint32_t> drp((size_t)nv + 1), dcol(ne ? ne : 1), dlev(nv);
-        ck(cudaMemcpyAsync(drp.ptr, rowptr, ((size_t)nv + 1) * 4u, cudaMemcpyHostToDevice, s), "graph upload");
-        if (ne) ck(cudaMemcpyAsync(dcol.ptr, col, ne * 4u, cudaMemcpyHostToDevice, s), "graph upload");
-        int rc = bfs_run(drp.ptr, dcol.ptr, nv, root, dlev.ptr, &cfg, res);
+        Staging& st = staging();
+        std::lock_guard<std::mutex> staged(st.lock);
+        uint32_t* drp = st.get<uint32_t>(0, (size_t)nv + 1);
+        uint32_t* dcol = st.get<uint32_t>(1, ne ? ne : 1);
+        uint32_t* dlev = st.get<uint32_t>(2, nv);
+        ck(cudaMemcpyAsync(drp, rowptr, ((size_t)nv + 1) * 4u, cudaMemcpyHostToDevice, s), "graph upload");
+        if (ne) ck(cudaMemcpyAsync(dcol, col, ne * 4u, cudaMemcpyHostToDevice, s), "graph upload");
+        int rc = bfs_run(drp, dcol, nv, root, dlev, &cfg, res);
         if (rc != HRM_OK) return rc;
-        ck(cudaMemcpyAsync(levels, dlev.ptr, (size_t)nv * 4u, cudaMemcpyDeviceToHost, s), "levels download");
+        ck(cudaMemcpyAsync(levels, dlev, (size_t)nv * 4u, cudaMemcpyDeviceToHost, s), "levels download");
         ck(cudaStreamSynchronize(s), "levels download");
         return HRM_OK;
     })

@@ -253,6 +253,8 @@ def main(argv=None):
     ap.add_argument("--photon-job", type=int, default=0)
     ap.add_argument("--variant", type=int, default=2)
     ap.add_argument("--arena", type=int, default=0)
+    ap.add_argument("--arm", choices=["persistent", "runtime", "plain"], default="persistent",
+                    help="one persistent launch, one single-spec runtime run per job, or one plain kernel per job")
     a = ap.parse_args(argv)
     if a.photon_job:
         specs = [{"kind": JOB_PHOTON, "first": 0, "count": a.photon_job, "seed": 0x1234567, "medium": 0}]
@@ -262,9 +264,17 @@ def main(argv=None):
         mix = Mix(make_mix_specs(a.jobs, seed=a.seed), photon_grid=32, media=8, seed=a.seed)
         kinds = {v: k for k, v in KIND_NAMES.items()}
         idx = None if a.kind is None else [i for i, s in enumerate(mix.specs) if s["kind"] == kinds[a.kind]]
-    done, res = batch_run(mix, 0, indices=idx, variant=a.variant, arena=a.arena)
+    if a.arm == "persistent":
+        batch_run(mix, 0, indices=idx, variant=a.variant, arena=a.arena)  # warm-up (graph capture)
+        done, res = batch_run(mix, 0, indices=idx, variant=a.variant, arena=a.arena)
+        res["calls_per_s"] = res["evals"] / (res["device_ms"] / 1e3)
+    else:
+        run = runtime_run if a.arm == "runtime" else plain_run
+        run(mix, 1, indices=idx)  # warm-up
+        done, ms = run(mix, 1, indices=idx)
+        res = {"total_ms": ms}
+    res["arm"] = a.arm
     res["jobs"] = len(done)
-    res["calls_per_s"] = res["evals"] / (res["device_ms"] / 1e3)
     print(json.dumps(res))
 
 

@@ -103,7 +103,10 @@ int hrm_set_device(int device);
 int hrm_device_sync(void);
 /* The whole-run helpers (hrm_*_run*) keep one program instance per device, spec, program
  * type, variant and arena size, re-initialised by each run, so repeated runs allocate no
- * device memory; concurrent runs on the same cached instance are serialised. This frees them. */
+ * device memory; concurrent runs on the same cached instance are serialised. The host-buffer
+ * runs (hrm_collatz_run, hrm_photon_run, hrm_bfs_run) likewise keep their device copies of
+ * inputs and outputs per device, grown on demand, and run one at a time per device. This
+ * frees both. */
 int hrm_release_cache(void);
 
 /* ---- program life cycle (templates.py:3-184 counterparts) ------------------------------
