@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--variant", type=int, default=-1, help="compiled tuning variant (-1 = autotuned)")
+    p.add_argument("--job-order", default="admission", choices=["admission", "round-robin"],
+                   help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
     return p.parse_args()
 
 
@@ -351,7 +353,7 @@ def run_batched(args):
     from harmonize_b200 import jobs
     specs = jobs.make_mix_specs(args.jobs, seed=1)
     mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1, sets=3)
-    tc = pick_config(args, "batched", "async")
+    tc = dict(pick_config(args, "batched", "async"), job_order=1 if args.job_order == "admission" else 0)
     variant = tc["variant"]
     warm = list(range(min(48, args.jobs)))
     jobs.batch_run(mix, 0, warm, **tc)
@@ -404,7 +406,7 @@ def run_serving(args):
     n = args.serve_jobs
     specs = jobs.make_mix_specs(n, seed=2)
     mix = jobs.Mix(specs, photon_grid=32, media=8, seed=2, sets=3)
-    tc = pick_config(args, "batched", "async")
+    tc = dict(pick_config(args, "batched", "async"), job_order=1 if args.job_order == "admission" else 0)
     variant = tc["variant"]
     done_b, res = jobs.batch_run(mix, 0, **tc)
     sat = n / (res["device_ms"] / 1e3)

@@ -122,6 +122,12 @@ __global__ void mix_prepare_range_kernel(JobRecord* jobs, unsigned int first, un
     }
 }
 
+// The order in which make_work serves jobs (hrm_run_config.job_order).
+unsigned int job_order_of(const hrm_run_config& cfg) {
+    if (cfg.job_order > HRM_JOB_ORDER_ADMISSION) throw std::invalid_argument("unknown job_order");
+    return cfg.job_order == HRM_JOB_ORDER_ADMISSION ? hrm_specs::JOB_ORDER_ADMISSION : hrm_specs::JOB_ORDER_ROUND_ROBIN;
+}
+
 // Asks a running exec to stop (the same request prog.halt_early() makes).
 __global__ void halt_kernel(hrm_rt::RuntimeControl* ctl) {
     if (threadIdx.x == 0) atomicOr(&ctl->flags, hrm_rt::EARLY_HALT_FLAG);
@@ -161,6 +167,7 @@ struct Batch : BatchBase {
         s.low = c + 5;
         s.started = c + 6;
         s.max_active = 256;
+        s.job_order = hrm_specs::JOB_ORDER_ROUND_ROBIN;
         s.done_host = nullptr;
         s.njobs = cap;
         return s;
@@ -180,9 +187,9 @@ struct Batch : BatchBase {
 
     // Captures: timestamp, output preparation, init<P>, exec<P> (the launches bake in the
     // instance's tunables, so a change of them re-captures).
-    void capture(size_t groups, size_t cycles, unsigned int patience, unsigned int fill_links) {
+    void capture(size_t groups, size_t cycles, unsigned int patience, unsigned int fill_links, unsigned int order) {
         if (graph && groups == graph_groups && cycles == graph_cycles && patience == inst.patience &&
-            fill_links == inst.fill_links)
+            fill_links == inst.fill_links && order == inst.device_state.job_order)
             return;
         if (graph) {
             cudaGraphExecDestroy(graph);
@@ -190,6 +197,7 @@ struct Batch : BatchBase {
         }
         inst.patience = patience;
         inst.fill_links = fill_links;
+        inst.device_state.job_order = order;
         P::resident_ctas();  // sets the kernel's shared-memory attribute outside the capture
         cudaGraph_t g;
         ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -211,7 +219,7 @@ struct Batch : BatchBase {
         size_t groups = cfg.groups ? cfg.groups : (size_t)1 << 30;
         size_t cycles = cfg.cycles ? cfg.cycles : ((size_t)1 << 24);
         size_t max_execs = cfg.max_execs ? cfg.max_execs : 4096;
-        capture(groups, cycles, cfg.patience, cfg.fill_links);
+        capture(groups, cycles, cfg.patience, cfg.fill_links, job_order_of(cfg));
         unsigned int ctr[8] = {n, 0u, 0u, 0u, closed0, 0u, 0u, 0u};
         ck(cudaMemcpyAsync(jobs.data(), recs.data(), sizeof(JobRecord) * n, cudaMemcpyHostToDevice, stream), "jobs");
         ck(cudaMemcpyAsync(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice, stream), "counters");
@@ -404,6 +412,7 @@ struct Server : ServerBase {
         inst.device_state = st;
         inst.patience = cfg.patience;
         inst.fill_links = cfg.fill_links;
+        inst.device_state.job_order = job_order_of(cfg);
         unsigned int ctr[8] = {0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
         ck(cudaMemcpy(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice), "counters");
         P::launch_init(inst, groups, exec_s);

@@ -30,6 +30,7 @@
 namespace hrm_specs {
 
 enum JobKind : unsigned int { JOB_COLLATZ = 0u, JOB_PHOTON = 1u, JOB_BFS = 2u };
+enum JobOrder : unsigned int { JOB_ORDER_ROUND_ROBIN = 0u, JOB_ORDER_ADMISSION = 1u };
 
 // One job per 128-byte-aligned record: records never share a cache line, so a team that
 // reads an admitted record cannot pull a not-yet-written neighbour into its SM's L1 (records
@@ -61,6 +62,7 @@ struct MixState {
     unsigned int* low;             // every job below this index has an exhausted source
     unsigned int* started;         // jobs that have received their first make_work
     unsigned int max_active;       // a job starts only while started - completed < max_active
+    unsigned int job_order;        // JOB_ORDER_ROUND_ROBIN or JOB_ORDER_ADMISSION (make_work)
     unsigned long long* done_host; // host-mapped: t_done of each job (0 = not done), or null
     unsigned int njobs;            // capacity of the job table
 };
@@ -405,7 +407,11 @@ struct MixSpec {
             }
             unsigned int span = admitted > low ? admitted - low : 1u;
             for (unsigned int tries = 0; tries < 64u; tries++) {
-                unsigned int c = low + atomicAdd(st.cursor, 1u) % span;
+                // Round robin spreads the teams over all jobs in progress (they share the
+                // GPU); admission order gives the oldest job with work left every team that
+                // asks, so jobs finish nearly one after another, each at nearly full speed.
+                unsigned int c = st.job_order == JOB_ORDER_ADMISSION ? low + tries
+                                                                      : low + atomicAdd(st.cursor, 1u) % span;
                 if (c >= admitted) break;
                 JobRecord& r = st.jobs[c];
                 if (!r.source.done() && *(volatile unsigned int*)&r.done == 0u) {

@@ -79,7 +79,13 @@ typedef struct hrm_run_config {
     uint32_t patience;         /* AsyncProgram coalescing threshold: scheduling steps a partial
                                   batch may wait without growing before it runs; 0 = 16 */
     uint32_t fill_links;       /* AsyncProgram links one fill takes from the arena; 0 = 2 */
+    uint32_t job_order;        /* batched and serving runs: HRM_JOB_ORDER_* (which job make_work serves) */
 } hrm_run_config;
+
+/* Job orders of batched and serving runs: round robin over the jobs in progress (they share
+ * the GPU), or admission order (the oldest job with work left gets every team that asks). */
+#define HRM_JOB_ORDER_ROUND_ROBIN 0u
+#define HRM_JOB_ORDER_ADMISSION 1u
 
 /* Compiled tuning variants: shared-memory ring per async function (in 32-promise links)
  * and 32-lane teams per CTA. EventProgram uses only the team count. */

@@ -14,11 +14,11 @@ def small_mix(hrm):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", [0, 1])
-def test_batch_equals_plain_equals_oracle(hrm, small_mix, variant):
+@pytest.mark.parametrize("variant,job_order", [(0, 0), (1, 0), (1, 1), (2, 1)])
+def test_batch_equals_plain_equals_oracle(hrm, small_mix, variant, job_order):
     from harmonize_b200 import jobs
     mix = small_mix
-    done_b, res = jobs.batch_run(mix, which=0, variant=variant)
+    done_b, res = jobs.batch_run(mix, which=0, variant=variant, job_order=job_order)
     done_p, total = jobs.plain_run(mix, which=1, streams=4)
     assert (done_b != np.iinfo(np.uint64).max).all()
     for i, s in enumerate(mix.specs):
