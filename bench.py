@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--variant", type=int, default=-1, help="compiled tuning variant (-1 = autotuned)")
     p.add_argument("--job-order", default="admission", choices=["admission", "round-robin"],
                    help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
+    p.add_argument("--solo-photons", type=int, default=1 << 15,
+                   help="batched: photon jobs at least this large also run alone (the persistent_solo arm)")
     return p.parse_args()
 
 
@@ -352,7 +354,7 @@ def run_batched(args):
     import harmonize_b200 as hrm
     from harmonize_b200 import jobs
     specs = jobs.make_mix_specs(args.jobs, seed=1)
-    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1, sets=3)
+    mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1, sets=4)
     tc = dict(pick_config(args, "batched", "async"), job_order=1 if args.job_order == "admission" else 0)
     variant = tc["variant"]
     warm = list(range(min(48, args.jobs)))
@@ -365,7 +367,9 @@ def run_batched(args):
         done_p, plain_ms = jobs.plain_run(mix, 1, streams=16)
         torch.cuda.synchronize()
         done_r, runtime_ms = jobs.runtime_run(mix, 2)
-    for other, name in ((1, "plain-kernel"), (2, "per-job runtime")):
+        torch.cuda.synchronize()
+        done_s, solo_ms, _ = jobs.batch_run_solo(mix, 3, solo_photons=args.solo_photons, **tc)
+    for other, name in ((1, "plain-kernel"), (2, "per-job runtime"), (3, "persistent with solo large jobs")):
         mism = [i for i in range(len(specs)) if not np.array_equal(mix.output(0, i), mix.output(other, i))]
         if mism:
             raise SystemExit(f"bench: {len(mism)} jobs differ between the persistent and {name} runs")
@@ -380,15 +384,20 @@ def run_batched(args):
                    "persistent": "one launch (CUDA graph) of AsyncProgram<MixSpec>",
                    "runtime_per_job": "one whole single-spec AsyncProgram run per job (init, exec until "
                                       "complete, synchronised), tuned variant per kind",
-                   "plain": "one hand-written plain kernel launch per job (one thread per item), 16 streams"},
+                   "plain": "one hand-written plain kernel launch per job (one thread per item), 16 streams",
+                   "persistent_solo": f"photon jobs of >= {args.solo_photons} photons one by one through the "
+                                      "single-spec runtime, all other jobs in one persistent launch"},
         "jobs_per_s": {"persistent": round(args.jobs / (span_b / 1e3), 1),
+                       "persistent_solo": round(args.jobs / (solo_ms / 1e3), 1),
                        "runtime_per_job": round(args.jobs / (runtime_ms / 1e3), 1),
                        "plain": round(args.jobs / (plain_ms / 1e3), 1)},
         "speedup_job_throughput": {"vs_runtime_per_job": round(runtime_ms / span_b, 3),
-                                   "vs_plain_kernels": round(plain_ms / span_b, 3)},
-        "completion_ms": {"persistent": percentiles_ms(done_b), "runtime_per_job": percentiles_ms(done_r),
-                          "plain": percentiles_ms(done_p)},
-        "outputs": "identical per job (persistent vs per-job runtime vs plain kernels)",
+                                   "vs_plain_kernels": round(plain_ms / span_b, 3),
+                                   "solo_vs_runtime_per_job": round(runtime_ms / solo_ms, 3),
+                                   "solo_vs_plain_kernels": round(plain_ms / solo_ms, 3)},
+        "completion_ms": {"persistent": percentiles_ms(done_b), "persistent_solo": percentiles_ms(done_s),
+                          "runtime_per_job": percentiles_ms(done_r), "plain": percentiles_ms(done_p)},
+        "outputs": "identical per job (all four arms)",
         "full_batch_fraction": round(res["full_batches"] / max(1, res["batches"]), 4),
         "clocks": clk.summary(),
     }

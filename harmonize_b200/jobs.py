@@ -208,6 +208,35 @@ def batch_run(mix, which=0, indices=None, **cfg_kw):
     return done, res.as_dict()
 
 
+def batch_run_solo(mix, which=0, solo_photons=1 << 15, indices=None, **cfg_kw):
+    """The batch with its largest jobs taken out of the persistent launch.
+
+    Photon jobs of at least `solo_photons` photons each fill the GPU on their own, so running
+    them among the other jobs gains them nothing and costs them the job indirection of the
+    multiplexing kernel (about half its speed on photon work). They run one after another
+    through the single-spec runtime, after one persistent launch of all the other jobs.
+    Returns (done_ns per job from the start of the batch, total ms, result of the persistent
+    launch or None)."""
+    idx = list(range(len(mix.specs))) if indices is None else list(indices)
+    solo = [i for i in idx if mix.specs[i]["kind"] == JOB_PHOTON and mix.specs[i]["count"] >= solo_photons]
+    solo_set = set(solo)
+    rest = [i for i in idx if i not in solo_set]
+    pos = {i: k for k, i in enumerate(idx)}
+    done = np.zeros(len(idx), dtype=np.uint64)
+    total_ms, res = 0.0, None
+    if rest:
+        d, res = batch_run(mix, which, indices=rest, **cfg_kw)
+        for k, i in enumerate(rest):
+            done[pos[i]] = d[k]
+        total_ms += res["device_ms"]
+    if solo:
+        d, ms = runtime_run(mix, which, indices=solo)
+        for k, i in enumerate(solo):
+            done[pos[i]] = d[k] + np.uint64(total_ms * 1e6)
+        total_ms += ms
+    return done, total_ms, res
+
+
 def runtime_run(mix, which=1, indices=None, program="async", variants=None):
     """One whole single-spec runtime run per job, in order (plain execution of the runtime).
     variants: per job kind (Collatz, photon, BFS), default the autotuner's choice for each.
