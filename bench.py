@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+JOB_ORDERS = {"round-robin": 0, "admission": 1, "small-first": 2}  # HRM_JOB_ORDER_*
 
 
 def parse():
@@ -51,7 +52,7 @@ def parse():
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--variant", type=int, default=-1, help="compiled tuning variant (-1 = autotuned)")
-    p.add_argument("--job-order", default="admission", choices=["admission", "round-robin"],
+    p.add_argument("--job-order", default="small-first", choices=list(JOB_ORDERS),
                    help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
     p.add_argument("--solo-photons", type=int, default=1 << 15,
                    help="batched: photon jobs at least this large also run alone (the persistent_solo arm)")
@@ -355,7 +356,7 @@ def run_batched(args):
     from harmonize_b200 import jobs
     specs = jobs.make_mix_specs(args.jobs, seed=1)
     mix = jobs.Mix(specs, photon_grid=32, media=8, seed=1, sets=4)
-    tc = dict(pick_config(args, "batched", "async"), job_order=1 if args.job_order == "admission" else 0)
+    tc = dict(pick_config(args, "batched", "async"), job_order=JOB_ORDERS[args.job_order])
     variant = tc["variant"]
     warm = list(range(min(48, args.jobs)))
     jobs.batch_run(mix, 0, warm, **tc)
@@ -415,7 +416,7 @@ def run_serving(args):
     n = args.serve_jobs
     specs = jobs.make_mix_specs(n, seed=2)
     mix = jobs.Mix(specs, photon_grid=32, media=8, seed=2, sets=3)
-    tc = dict(pick_config(args, "batched", "async"), job_order=1 if args.job_order == "admission" else 0)
+    tc = dict(pick_config(args, "batched", "async"), job_order=JOB_ORDERS[args.job_order])
     variant = tc["variant"]
     done_b, res = jobs.batch_run(mix, 0, **tc)
     sat = n / (res["device_ms"] / 1e3)

@@ -113,7 +113,7 @@ def tune_batched(table, reps):
         best = 0.0
         try:
             for _ in range(reps + 1):
-                _, res = jobs.batch_run(mix, 0, job_order=1, **cand)  # admission order, as bench.py
+                _, res = jobs.batch_run(mix, 0, job_order=2, **cand)  # small first, as bench.py
                 best = max(best, n / (res["device_ms"] / 1e3))
         except Exception as e:
             sweep.append(dict(cand, error=str(e)))

@@ -30,7 +30,7 @@
 namespace hrm_specs {
 
 enum JobKind : unsigned int { JOB_COLLATZ = 0u, JOB_PHOTON = 1u, JOB_BFS = 2u };
-enum JobOrder : unsigned int { JOB_ORDER_ROUND_ROBIN = 0u, JOB_ORDER_ADMISSION = 1u };
+enum JobOrder : unsigned int { JOB_ORDER_ROUND_ROBIN = 0u, JOB_ORDER_ADMISSION = 1u, JOB_ORDER_SMALL_FIRST = 2u };
 
 // One job per 128-byte-aligned record: records never share a cache line, so a team that
 // reads an admitted record cannot pull a not-yet-written neighbour into its SM's L1 (records
@@ -43,7 +43,8 @@ struct alignas(128) JobRecord {
     unsigned long long t_admit;                  // %globaltimer when first worked on
     unsigned long long t_done;                   // %globaltimer at completion
     util::iter::AtomicIter<unsigned int> source; // the job's start values / photon ids / root
-    unsigned int pad[2];
+    unsigned int large;                          // 1: large job, served last by JOB_ORDER_SMALL_FIRST
+    unsigned int pad;
     union State {
         CollatzState c;
         PhotonState p;
@@ -406,14 +407,25 @@ struct MixSpec {
                 low = atomicCAS(st.low, low, low + 1u) == low ? low + 1u : *(volatile unsigned int*)st.low;
             }
             unsigned int span = admitted > low ? admitted - low : 1u;
-            for (unsigned int tries = 0; tries < 64u; tries++) {
-                // Round robin spreads the teams over all jobs in progress (they share the
-                // GPU); admission order gives the oldest job with work left every team that
-                // asks, so jobs finish nearly one after another, each at nearly full speed.
-                unsigned int c = st.job_order == JOB_ORDER_ADMISSION ? low + tries
-                                                                      : low + atomicAdd(st.cursor, 1u) % span;
-                if (c >= admitted) break;
+            // Round robin spreads the teams over all jobs in progress (they share the GPU);
+            // admission order gives the oldest job with work left every team that asks, so
+            // jobs finish nearly one after another, each at nearly full speed; small first
+            // does the same among the small jobs, and serves large ones when no small job has
+            // work left to start.
+            const bool rr = st.job_order == JOB_ORDER_ROUND_ROBIN;
+            const unsigned int passes = st.job_order == JOB_ORDER_SMALL_FIRST ? 2u : 1u;
+            for (unsigned int tries = 0; tries < 64u * passes && j == 0xFFFFFFFFu; tries++) {
+                const bool small_only = passes == 2u && tries < 64u;
+                unsigned int c = rr ? low + atomicAdd(st.cursor, 1u) % span : low + (tries & 63u);
+                if (c >= admitted) {
+                    if (small_only) {
+                        tries = 63u;  // on to the second pass
+                        continue;
+                    }
+                    break;
+                }
                 JobRecord& r = st.jobs[c];
+                if (small_only && r.large) continue;
                 if (!r.source.done() && *(volatile unsigned int*)&r.done == 0u) {
                     if (*(volatile unsigned long long*)&r.t_admit == 0ull) {
                         // Not started yet: start it only while fewer than max_active jobs

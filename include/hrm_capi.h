@@ -83,9 +83,12 @@ typedef struct hrm_run_config {
 } hrm_run_config;
 
 /* Job orders of batched and serving runs: round robin over the jobs in progress (they share
- * the GPU), or admission order (the oldest job with work left gets every team that asks). */
+ * the GPU), admission order (the oldest job with work left gets every team that asks), or
+ * small first (admission order among the jobs estimated to need fewer than about 5e7 async
+ * calls, then among all). */
 #define HRM_JOB_ORDER_ROUND_ROBIN 0u
 #define HRM_JOB_ORDER_ADMISSION 1u
+#define HRM_JOB_ORDER_SMALL_FIRST 2u
 
 /* Compiled tuning variants: shared-memory ring per async function (in 32-promise links)
  * and 32-lane teams per CTA. EventProgram uses only the team count. */

@@ -14,7 +14,7 @@ def small_mix(hrm):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant,job_order", [(0, 0), (1, 0), (1, 1), (2, 1)])
+@pytest.mark.parametrize("variant,job_order", [(0, 0), (1, 0), (1, 1), (2, 1), (2, 2)])
 def test_batch_equals_plain_equals_oracle(hrm, small_mix, variant, job_order):
     from harmonize_b200 import jobs
     mix = small_mix

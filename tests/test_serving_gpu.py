@@ -37,12 +37,12 @@ def test_server_results_same_alone_and_in_mix(hrm, mix):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["resident", "plain"])
-def test_replay_completes_every_job(hrm, mix, mode):
+@pytest.mark.parametrize("mode,job_order", [("resident", 0), ("resident", 2), ("runtime", 0), ("plain", 0)])
+def test_replay_completes_every_job(hrm, mix, mode, job_order):
     from harmonize_b200 import jobs
     n = len(mix.specs)
     arrivals = jobs.poisson_arrivals(n, rate_per_s=20000.0, seed=3)
-    lat, span = jobs.serve_replay(mix, arrivals, mode=mode, which=0, streams=4, arena=1 << 18)
+    lat, span = jobs.serve_replay(mix, arrivals, mode=mode, which=0, streams=4, arena=1 << 18, job_order=job_order)
     assert (lat > 0).all() and span > 0
     ref = [mix.output(0, i).copy() for i in range(n)]
     jobs.plain_run(mix, which=1, streams=4)
