@@ -14,8 +14,11 @@ e2e   : the same metric through the host-buffer entry point (hrm_*_run): input u
         result download inside the timed region, pinned host memory.
 --gpus N under torchrun: one independent replica per GPU (the walk has no cross-replica
 exchange), photon ids offset per rank (weak scaling); time = max over ranks.
---impl reference: the reference runtime (Harmonize's own AsyncProgram, built from its
-headers with the same spec source into oracle/_ref) on the same workload and metric.
+--impl reference: the reference runtime (Harmonize's own runtime built from its headers with
+the same spec source into oracle/_ref: its EventProgram for the photon walk, on which its
+AsyncProgram faulted) on the same workload and metric, over a bounded sample per step.
+--workload batched / serving: the job mix in the persistent runtime against one single-spec
+runtime run per job and one plain kernel per job (see run_batched / run_serving).
 """
 import argparse
 import ctypes

@@ -6,7 +6,12 @@ The runtime itself is C++/CUDA (``include/harmonize.h``); this module loads the 
   * ``Program``: the instance life cycle of the original's foreign-call shim
     (alloc_program / init_program / exec_program / complete / clear_flags / free_program,
     harmonize/python/templates.py:3-184) for the built-in specs;
-  * whole runs of the built-in specs from host arrays: ``collatz``.
+  * whole runs of the built-in specs from host arrays: ``collatz``, ``photon_walk``, ``bfs``,
+    ``barrier_demo``; seeded inputs ``photon_medium`` and ``rmat_csr``;
+  * ``harmonize_b200.jobs``: many jobs in one persistent launch (``batch_run``,
+    ``batch_run_solo``), a resident serving session (``Server``, ``serve_replay``) and the
+    per-job baselines (``runtime_run``, ``plain_run``);
+  * ``harmonize_b200.autotune``: the tuner behind ``tuned.json``.
 
 There is no CPU fallback: if the library or a GPU is missing, calls raise.
 """
