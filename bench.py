@@ -59,6 +59,8 @@ def parse():
                    help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
     p.add_argument("--solo-photons", type=int, default=1 << 15,
                    help="batched: photon jobs at least this large also run alone (the persistent_solo arm)")
+    p.add_argument("--serve-solo-photons", type=int, default=1 << 17,
+                   help="serving: photon jobs at least this large run alone (0 = never)")
     return p.parse_args()
 
 
@@ -427,7 +429,8 @@ def run_serving(args):
     for frac in args.rates:
         rate = frac * sat
         arr = jobs.poisson_arrivals(n, rate, seed=5)
-        lat_r, span_r = jobs.serve_replay(mix, arr, mode="resident", which=0, **tc)
+        lat_r, span_r = jobs.serve_replay(mix, arr, mode="resident", which=0, solo_photons=args.serve_solo_photons,
+                                          **tc)
         lat_p, span_p = jobs.serve_replay(mix, arr, mode="plain", which=1, streams=16)
         lat_u, span_u = jobs.serve_replay(mix, arr, mode="runtime", which=2)
         rows.append({"load": frac, "rate_jobs_per_s": round(rate, 1),

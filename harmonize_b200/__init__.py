@@ -49,7 +49,8 @@ class RunConfig(ctypes.Structure):
     _fields_ = [("program_type", ctypes.c_int), ("groups", ctypes.c_size_t), ("cycles", ctypes.c_size_t),
                 ("chunk", ctypes.c_size_t), ("arena", ctypes.c_size_t), ("max_execs", ctypes.c_size_t),
                 ("stream", ctypes.c_void_p), ("variant", ctypes.c_int), ("patience", ctypes.c_uint32),
-                ("fill_links", ctypes.c_uint32), ("job_order", ctypes.c_uint32)]
+                ("fill_links", ctypes.c_uint32), ("job_order", ctypes.c_uint32),
+                ("solo_photons", ctypes.c_uint32)]
 
 
 # Compiled tuning variants: (shared-memory ring links per function, teams per CTA).
@@ -129,9 +130,10 @@ def exported_symbols():
 
 
 def make_config(program="async", groups=0, cycles=0, chunk=0, arena=0, max_execs=0, stream=None, variant=0,
-                patience=0, fill_links=0, job_order=0):
+                patience=0, fill_links=0, job_order=0, solo_photons=0):
     pt = {"async": ASYNC, "event": EVENT}[program] if isinstance(program, str) else int(program)
-    return RunConfig(pt, groups, cycles, chunk, arena, max_execs, stream, variant, patience, fill_links, job_order)
+    return RunConfig(pt, groups, cycles, chunk, arena, max_execs, stream, variant, patience, fill_links, job_order,
+                     solo_photons)
 
 
 def collatz(start, count, program="async", **kw):

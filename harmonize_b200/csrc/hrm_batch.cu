@@ -18,6 +18,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstddef>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -119,6 +120,15 @@ __global__ void mix_prepare_kernel(JobRecord* jobs, const unsigned int* admitted
 
 __global__ void stamp_kernel(unsigned long long* t) {
     if (threadIdx.x == 0) *t = hrm_specs::global_ns();
+}
+
+// Completion stamp of a job served outside the persistent kernel, into the host-mapped array.
+__global__ void stamp_done_kernel(unsigned long long* done, unsigned int j) {
+    if (threadIdx.x == 0) {
+        volatile unsigned long long* d = done;
+        d[j] = hrm_specs::global_ns();
+        __threadfence_system();
+    }
 }
 
 // Clears the outputs of jobs [first, first+n) before they are published to a running kernel.
@@ -406,6 +416,17 @@ struct Server : ServerBase {
     std::mutex err_lock;
     std::string err;
     size_t arena_links;
+    // Solo lane: photon jobs of at least solo_photons photons fill the GPU on their own and run
+    // at about half speed inside the multiplexing kernel, so the session serves them alone
+    // through the single-spec runtime: submit queues them and halts the running exec (teams
+    // spill their work and leave within a few scheduling rounds); the runner serves the queue
+    // in submission order between execs, then resumes the persistent kernel, whose state
+    // waited in the arena. Their job records are placeholders with an empty source, which the
+    // kernel closes and never works on.
+    unsigned int solo_photons;
+    std::mutex solo_lock;
+    std::deque<std::pair<unsigned int, hrm_job>> solo_queue;  // (job index, job)
+    unsigned long long* done_dev = nullptr;                    // device alias of done_host
 
     Server(unsigned int cap, const hrm_run_config& cfg)
         : inst((typename P::AdrType)(cfg.arena ? cfg.arena : ((size_t)1 << 21)), MixState{}),
@@ -414,10 +435,10 @@ struct Server : ServerBase {
           capacity(cap),
           groups(cfg.groups ? cfg.groups : (size_t)1 << 30),
           cycles(cfg.cycles ? cfg.cycles : ((size_t)1 << 20)),
-          arena_links(cfg.arena ? cfg.arena : ((size_t)1 << 21)) {
+          arena_links(cfg.arena ? cfg.arena : ((size_t)1 << 21)),
+          solo_photons(cfg.solo_photons) {
         ck(cudaHostAlloc((void**)&done_host, sizeof(unsigned long long) * cap, cudaHostAllocMapped), "done flags");
         memset(done_host, 0, sizeof(unsigned long long) * cap);
-        unsigned long long* done_dev = nullptr;
         ck(cudaHostGetDevicePointer((void**)&done_dev, done_host, 0), "done flags device alias");
         ck(cudaHostAlloc((void**)&staging, sizeof(JobRecord) * 4096, cudaHostAllocDefault), "staging");
         ck(cudaHostAlloc((void**)&pinned_ctr, sizeof(unsigned int) * 8, cudaHostAllocDefault), "staging");
@@ -440,6 +461,7 @@ struct Server : ServerBase {
         cudaFuncAttributes fa;
         ck(cudaFuncGetAttributes(&fa, mix_prepare_range_kernel), "kernel load");
         ck(cudaFuncGetAttributes(&fa, halt_kernel), "kernel load");
+        ck(cudaFuncGetAttributes(&fa, stamp_done_kernel), "kernel load");
         mix_prepare_range_kernel<<<1, 32, 0, submit_s>>>(jobs.data(), 0u, 0u);
         ck(cudaGetLastError(), "kernel load");
         ck(cudaStreamSynchronize(submit_s), "kernel load");
@@ -467,15 +489,55 @@ struct Server : ServerBase {
     }
 
     // Relaunches the persistent kernel until the session is closed and every job is done.
+    bool pop_solo(std::pair<unsigned int, hrm_job>& out) {
+        std::lock_guard<std::mutex> g(solo_lock);
+        if (solo_queue.empty()) return false;
+        out = solo_queue.front();
+        solo_queue.pop_front();
+        return true;
+    }
+
+    // One queued solo job, on the exec stream while the persistent kernel is not running.
+    void run_solo(unsigned int j, const hrm_job& jb) {
+        hrm_run_config c;
+        memset(&c, 0, sizeof(c));
+        c.program_type = HRM_ASYNC;
+        c.variant = HRM_VARIANT_R4_T2;  // the photon walk's tuned variant on this GPU
+        c.stream = exec_s;
+        hrm_run_result r;
+        if (hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
+                                  jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
+            throw std::runtime_error(std::string("solo photon job: ") + hrm_last_error());
+        stamp_done_kernel<<<1, 32, 0, exec_s>>>(done_dev, j);
+        ck(cudaGetLastError(), "solo stamp");
+        ck(cudaStreamSynchronize(exec_s), "solo stamp");
+    }
+
     void loop() {
         try {
             while (true) {
+                if (stop) break;
+                // Clear a served halt request, then look at the solo queue: submit queues a
+                // job before it requests the halt, so a job queued after this look comes with
+                // a halt that lands after this clear and stops the exec launched below.
+                ck(cudaMemsetAsync(&inst.control.data()->flags, 0, sizeof(unsigned int), exec_s), "clear flags");
+                ck(cudaStreamSynchronize(exec_s), "clear flags");
+                std::pair<unsigned int, hrm_job> sj;
+                if (pop_solo(sj)) {
+                    run_solo(sj.first, sj.second);
+                    continue;
+                }
                 P::launch_exec(inst, groups, cycles, exec_s);
                 ck(cudaStreamSynchronize(exec_s), "serving exec");
                 unsigned int f = inst.flags();
                 if (f & hrm_rt::ERROR_MASK) hrm_rt::throw_flags(f);
                 if (stop) break;
-                if (!host_open && (f & hrm_rt::COMPLETION_FLAG)) break;
+                bool solo_left;
+                {
+                    std::lock_guard<std::mutex> g(solo_lock);
+                    solo_left = !solo_queue.empty();
+                }
+                if (!host_open && (f & hrm_rt::COMPLETION_FLAG) && !solo_left) break;
             }
         } catch (std::exception& e) {
             std::lock_guard<std::mutex> g(err_lock);
@@ -486,12 +548,20 @@ struct Server : ServerBase {
     unsigned int submit(const hrm_job* in, unsigned int n) override {
         if (submitted + n > capacity) throw std::invalid_argument("server job table is full");
         unsigned int first = submitted;
+        std::vector<std::pair<unsigned int, hrm_job>> solo;
         for (unsigned int done = 0; done < n;) {
             unsigned int k = std::min(n - done, 4096u);
             for (unsigned int i = 0; i < k; i++) {
-                if (job_sources(in[done + i]) == 0) throw std::invalid_argument("a served job needs work to do");
-                validate(in[done + i]);
-                staging[i] = make_record(in[done + i], jobs.data() + first + done + i);
+                const hrm_job& jb = in[done + i];
+                if (job_sources(jb) == 0) throw std::invalid_argument("a served job needs work to do");
+                validate(jb);
+                staging[i] = make_record(jb, jobs.data() + first + done + i);
+                if (solo_photons && jb.kind == HRM_JOB_PHOTON && jb.count >= solo_photons) {
+                    // Placeholder: an empty source, already done; the kernel closes it.
+                    staging[i].source = util::iter::AtomicIter<unsigned int>(jb.first, jb.first);
+                    staging[i].done = 1;
+                    solo.emplace_back(first + done + i, jb);
+                }
             }
             ck(cudaMemcpyAsync(jobs.data() + first + done, staging, sizeof(JobRecord) * k, cudaMemcpyHostToDevice,
                                submit_s), "job records");
@@ -505,6 +575,16 @@ struct Server : ServerBase {
         ck(cudaMemcpyAsync(counters.data(), pinned_ctr, 4, cudaMemcpyHostToDevice, submit_s), "admit");
         ck(cudaStreamSynchronize(submit_s), "admit");
         submitted = first + n;
+        if (!solo.empty()) {
+            {
+                std::lock_guard<std::mutex> g(solo_lock);
+                for (auto& s : solo) solo_queue.push_back(s);
+            }
+            // Queued first, then the halt: see loop().
+            halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
+            ck(cudaGetLastError(), "solo halt");
+            ck(cudaStreamSynchronize(submit_s), "solo halt");
+        }
         return first;
     }
 

@@ -403,7 +403,14 @@ struct MixSpec {
             // Advance the low watermark past jobs whose sources are exhausted, then probe
             // round robin among [low, admitted).
             unsigned int low = *(volatile unsigned int*)st.low;
-            while (low < admitted && *(volatile unsigned int*)&st.jobs[low].source_closed) {
+            while (low < admitted) {
+                JobRecord& lr = st.jobs[low];
+                if (*(volatile unsigned int*)&lr.source_closed == 0u) {
+                    // A job whose source is exhausted but that no make_work closed yet (one
+                    // the host serves outside this kernel arrives that way) is closed here.
+                    if (!lr.source.done()) break;
+                    if (atomicCAS(&lr.source_closed, 0u, 1u) == 0u) atomicAdd(st.closed, 1u);
+                }
                 low = atomicCAS(st.low, low, low + 1u) == low ? low + 1u : *(volatile unsigned int*)st.low;
             }
             unsigned int span = admitted > low ? admitted - low : 1u;

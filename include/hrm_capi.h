@@ -80,6 +80,9 @@ typedef struct hrm_run_config {
                                   batch may wait without growing before it runs; 0 = 16 */
     uint32_t fill_links;       /* AsyncProgram links one fill takes from the arena; 0 = 2 */
     uint32_t job_order;        /* batched and serving runs: HRM_JOB_ORDER_* (which job make_work serves) */
+    uint32_t solo_photons;     /* serving sessions: photon jobs of at least this many photons run
+                                  alone through the single-spec runtime (the resident kernel
+                                  pauses meanwhile); 0 = never */
 } hrm_run_config;
 
 /* Job orders of batched and serving runs: round robin over the jobs in progress (they share

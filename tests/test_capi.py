@@ -86,7 +86,7 @@ def test_ctypes_structs_match_the_c_layout(hrm, tmp_path):
                    'int main(void) {\n'
                    '  printf("%zu %zu %zu %zu\\n", sizeof(hrm_run_config), offsetof(hrm_run_config, variant),\n'
                    '         offsetof(hrm_run_config, patience), offsetof(hrm_run_config, fill_links));\n'
-                   '  printf("%zu\\n", offsetof(hrm_run_config, job_order));\n'
+                   '  printf("%zu %zu\\n", offsetof(hrm_run_config, job_order), offsetof(hrm_run_config, solo_photons));\n'
                    '  printf("%zu %zu\\n", sizeof(hrm_run_result), offsetof(hrm_run_result, device_ms));\n'
                    '  printf("%zu %zu\\n", sizeof(hrm_job), offsetof(hrm_job, out));\n'
                    '  return 0;\n}\n')
@@ -97,6 +97,6 @@ def test_ctypes_structs_match_the_c_layout(hrm, tmp_path):
     got = [list(map(int, line.split())) for line in subprocess.check_output([str(exe)], text=True).splitlines()]
     C = hrm.RunConfig
     assert got[0] == [ctypes.sizeof(C), C.variant.offset, C.patience.offset, C.fill_links.offset]
-    assert got[1] == [C.job_order.offset]
+    assert got[1] == [C.job_order.offset, C.solo_photons.offset]
     assert got[2] == [ctypes.sizeof(hrm.RunResult), hrm.RunResult.device_ms.offset]
     assert got[3] == [ctypes.sizeof(jobs.Job), jobs.Job.out.offset]

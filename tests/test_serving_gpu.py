@@ -51,6 +51,22 @@ def test_replay_completes_every_job(hrm, mix, mode, job_order):
 
 
 @pytest.mark.gpu
+def test_replay_with_solo_photon_jobs(hrm, mix):
+    """Large photon jobs served alone (the resident kernel pauses): every job completes and
+    every output equals one plain launch per job."""
+    from harmonize_b200 import jobs
+    n = len(mix.specs)
+    counts = sorted(s["count"] for s in mix.specs if s["kind"] == jobs.JOB_PHOTON)
+    arrivals = jobs.poisson_arrivals(n, rate_per_s=5000.0, seed=4)
+    lat, span = jobs.serve_replay(mix, arrivals, mode="resident", which=0, arena=1 << 18, job_order=2,
+                                  solo_photons=counts[len(counts) // 2])
+    assert (lat > 0).all() and span > 0
+    jobs.plain_run(mix, which=1, streams=4)
+    for i, s in enumerate(mix.specs):
+        assert np.array_equal(mix.output(0, i), mix.output(1, i)), (i, s)
+
+
+@pytest.mark.gpu
 def test_server_rejects_empty_jobs(hrm, mix):
     from harmonize_b200 import jobs
     arr = mix.job_array(0, [0])
