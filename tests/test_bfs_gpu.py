@@ -41,3 +41,16 @@ def test_bfs_isolated_root(hrm):
     exp = np.full(8, 0xFFFFFFFF, dtype=np.uint32)
     exp[3] = 0
     assert np.array_equal(levels, exp)
+
+
+@pytest.mark.gpu
+def test_arena_exhaustion_is_reported_and_the_next_run_is_sound(hrm, rmat14):
+    """One CTA and an arena of 32 links for a frontier of thousands of vertices: the device
+    raises ARENA_EXHAUSTED, the run ends with an error status instead of waiting, and the next
+    run, on an arena of the default size, is exact."""
+    rp, col = rmat14
+    with pytest.raises(hrm.HarmonizeError) as err:
+        hrm.bfs(rp, col, 0, program="async", groups=1, arena=32)
+    assert err.value.code == hrm.HRM_EDEVICE and "ARENA_EXHAUSTED" in str(err.value)
+    levels, _ = hrm.bfs(rp, col, 0, program="async")
+    assert np.array_equal(levels, oracle.bfs(rp, col, 0))
