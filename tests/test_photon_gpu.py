@@ -37,3 +37,21 @@ def test_photon_zero_photons(hrm, medium16):
     mu, ab, sp = medium16
     tally, res = hrm.photon_walk(mu, ab, sp, 16, 1, 0, 0)
     assert not tally.any() and res["evals"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", range(5))
+def test_every_compiled_variant_matches_oracle(hrm, medium16, variant):
+    """Every compiled tuning variant (ring links per function, teams per CTA) gives
+    the same tallies and call count for all three specs."""
+    assert variant in hrm.VARIANTS
+    mu, ab, sp = medium16
+    for program in ("async", "event"):
+        tally, res = hrm.photon_walk(mu, ab, sp, 16, 0xC0FFEE, 5, 2000, program=program, variant=variant)
+        ref, calls = oracle.photon_walk(mu, ab, sp, 16, 0xC0FFEE, 5, 2000)
+        assert np.array_equal(tally, ref) and res["evals"] == int(calls.sum())
+        steps, _ = hrm.collatz(1, 5000, program=program, variant=variant)
+        assert np.array_equal(steps, oracle.collatz_range(1, 5000))
+        rp, col = hrm.rmat_csr(12, 8, seed=5)
+        levels, _ = hrm.bfs(rp, col, 0, program=program, variant=variant)
+        assert np.array_equal(levels, oracle.bfs(rp, col, 0))
