@@ -104,17 +104,28 @@ struct PhotonTally {
     }
 };
 
-// Distance along direction component d from coordinate x to the face of [lo, lo+1).
+// Distance along direction component d from coordinate x to the face of [lo, lo+1) that
+// the photon is heading for (the upper face for d > 0, the lower one for d < 0). One
+// division whatever the sign, so that the lanes of a warp with mixed signs share it.
 HRM_HD HRM_FI float face_distance(float x, float d, unsigned int lo) {
-    if (d > 0.0f) {
-        float t = hrm::fdiv(hrm::fsub((float)(lo + 1u), x), d);
-        return t > 0.0f ? t : 0.0f;
-    }
-    if (d < 0.0f) {
-        float t = hrm::fdiv(hrm::fsub((float)lo, x), d);
-        return t > 0.0f ? t : 0.0f;
-    }
-    return 3.0e38f;
+    const bool up = d > 0.0f;
+    if (!up && !(d < 0.0f)) return 3.0e38f;  // d is zero (or NaN): no face ahead
+    const float face = (float)(up ? lo + 1u : lo);
+    const float t = hrm::fdiv(hrm::fsub(face, x), d);
+    return t > 0.0f ? t : 0.0f;
+}
+
+// Id of child c (0 or 1) of photon `id` split at step `step`.
+HRM_HD HRM_FI unsigned long long child_id(unsigned long long id, unsigned int step, unsigned int c) {
+    return hrm::mix64(id ^ (((unsigned long long)step << 1) | c) * 0x9E3779B97F4A7C15ull);
+}
+
+// Voxel index -> (ix, iy, iz) with two divisions: v / (n*n) == (v / n) / n for unsigned v.
+HRM_HD HRM_FI void voxel_coords(unsigned int v, unsigned int n, unsigned int& ix, unsigned int& iy, unsigned int& iz) {
+    const unsigned int q = v / n;
+    ix = v - q * n;
+    iz = q / n;
+    iy = q - iz * n;
 }
 
 struct PhotonMove {
@@ -123,7 +134,8 @@ struct PhotonMove {
     HRM_DEV static void eval(PROGRAM prog, Photon p) {
         const PhotonState& s = prog.device;
         const unsigned int n = s.n;
-        unsigned int ix = p.voxel % n, iy = (p.voxel / n) % n, iz = p.voxel / (n * n);
+        unsigned int ix, iy, iz;
+        voxel_coords(p.voxel, n, ix, iy, iz);
         float mu = s.mu_s[p.voxel];
         hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_MOVE);
         float dist = hrm::fdiv(hrm::fsub(0.0f, hrm::log_exact(hrm::u01_open0(r.x))), mu);
@@ -145,36 +157,41 @@ struct PhotonMove {
         p.x = hrm::fadd(p.x, hrm::fmul(tb, p.dx));
         p.y = hrm::fadd(p.y, hrm::fmul(tb, p.dy));
         p.z = hrm::fadd(p.z, hrm::fmul(tb, p.dz));
-        // Land exactly on the face and step the voxel index along the crossing axis.
-        bool out = false;
-        if (axis == 0) {
-            if (p.dx > 0.0f) { p.x = (float)(ix + 1u); out = (ix + 1u == n); ix += 1u; }
-            else { p.x = (float)ix; out = (ix == 0u); ix -= 1u; }
-        } else if (axis == 1) {
-            if (p.dy > 0.0f) { p.y = (float)(iy + 1u); out = (iy + 1u == n); iy += 1u; }
-            else { p.y = (float)iy; out = (iy == 0u); iy -= 1u; }
-        } else {
-            if (p.dz > 0.0f) { p.z = (float)(iz + 1u); out = (iz + 1u == n); iz += 1u; }
-            else { p.z = (float)iz; out = (iz == 0u); iz -= 1u; }
-        }
+        // Land exactly on the face and step the voxel index along the crossing axis (written
+        // with selects, so that the lanes of a warp crossing different faces do not diverge).
+        const float d_axis = axis == 0 ? p.dx : (axis == 1 ? p.dy : p.dz);
+        const unsigned int c = axis == 0 ? ix : (axis == 1 ? iy : iz);
+        const bool up = d_axis > 0.0f;
+        const float face = (float)(up ? c + 1u : c);
+        const bool out = up ? (c + 1u == n) : (c == 0u);
+        const unsigned int c_next = up ? c + 1u : c - 1u;
+        if (axis == 0) { p.x = face; ix = c_next; }
+        else if (axis == 1) { p.y = face; iy = c_next; }
+        else { p.z = face; iz = c_next; }
         if (out) {
             prog.template async<PhotonTally>(n * n * n + (p.id_lo & (PHOTON_SPREAD - 1u)), to_fixed(p.w));
             return;
         }
         p.voxel = ix + n * (iy + n * iz);
-        if (s.split[p.voxel]) {
-            p.w = hrm::fmul(p.w, 0.5f);
-            unsigned long long id = ((unsigned long long)p.id_hi << 32) | p.id_lo;
-            for (unsigned int c = 0; c < 2u; c++) {
-                unsigned long long cid = hrm::mix64(id ^ (((unsigned long long)p.step << 1) | c) * 0x9E3779B97F4A7C15ull);
-                Photon q = p;
-                q.id_lo = (unsigned int)cid;
-                q.id_hi = (unsigned int)(cid >> 32);
-                prog.template async<PhotonMove>(q);
-            }
-            return;
+        // Entering a flagged voxel splits the photon into two children of half weight. The
+        // first call below is the photon itself or its first child, the second one the
+        // second child, so that a warp with and without splits makes two calls, not three.
+        const bool split = s.split[p.voxel] != 0;
+        const unsigned long long id = ((unsigned long long)p.id_hi << 32) | p.id_lo;
+        Photon q = p;
+        if (split) {
+            q.w = hrm::fmul(p.w, 0.5f);
+            const unsigned long long cid = child_id(id, p.step, 0u);
+            q.id_lo = (unsigned int)cid;
+            q.id_hi = (unsigned int)(cid >> 32);
         }
-        prog.template async<PhotonMove>(p);
+        prog.template async<PhotonMove>(q);
+        if (split) {
+            const unsigned long long cid = child_id(id, p.step, 1u);
+            q.id_lo = (unsigned int)cid;
+            q.id_hi = (unsigned int)(cid >> 32);
+            prog.template async<PhotonMove>(q);
+        }
     }
 };
 
@@ -188,17 +205,16 @@ struct PhotonCollide {
         p.w = hrm::fsub(p.w, dep);
         prog.template async<PhotonTally>(p.voxel, to_fixed(dep));
         if (p.w < WEIGHT_CUTOFF) {
+            // Russian roulette: a survivor tallies the weight it gains, a loser the weight it
+            // loses (one call site for both, so that a warp of both kinds makes one call).
             hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_ROULETTE);
-            unsigned int spread = p.id_lo & (PHOTON_SPREAD - 1u);
-            if (hrm::u01_open0(r.x) <= ROULETTE_SURVIVAL) {
-                float boosted = hrm::fmul(p.w, ROULETTE_BOOST);
-                prog.template async<PhotonTally>(n * n * n + 2u * PHOTON_SPREAD + spread,
-                                                 to_fixed(hrm::fsub(boosted, p.w)));
-                p.w = boosted;
-            } else {
-                prog.template async<PhotonTally>(n * n * n + PHOTON_SPREAD + spread, to_fixed(p.w));
-                return;
-            }
+            const unsigned int spread = p.id_lo & (PHOTON_SPREAD - 1u);
+            const bool survive = hrm::u01_open0(r.x) <= ROULETTE_SURVIVAL;
+            const float boosted = hrm::fmul(p.w, ROULETTE_BOOST);
+            const unsigned int slot = n * n * n + (survive ? 2u : 1u) * PHOTON_SPREAD + spread;
+            prog.template async<PhotonTally>(slot, survive ? to_fixed(hrm::fsub(boosted, p.w)) : to_fixed(p.w));
+            if (!survive) return;
+            p.w = boosted;
         }
         isotropic(s, p.id_lo, p.id_hi, p.step, p.dx, p.dy, p.dz);
         p.step += 1u;
@@ -244,7 +260,8 @@ HRM_HD HRM_FI bool photon_walk_thread(const PhotonState& s, unsigned int id, uns
         Photon p = stack[--top];
         while (true) {
             k++;  // move
-            unsigned int ix = p.voxel % n, iy = (p.voxel / n) % n, iz = p.voxel / (n * n);
+            unsigned int ix, iy, iz;
+            voxel_coords(p.voxel, n, ix, iy, iz);
             hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_MOVE);
             float dist = hrm::fdiv(hrm::fsub(0.0f, hrm::log_exact(hrm::u01_open0(r.x))), s.mu_s[p.voxel]);
             float tx = face_distance(p.x, p.dx, ix);
@@ -305,8 +322,7 @@ HRM_HD HRM_FI bool photon_walk_thread(const PhotonState& s, unsigned int id, uns
                 p.w = hrm::fmul(p.w, 0.5f);
                 unsigned long long id64 = ((unsigned long long)p.id_hi << 32) | p.id_lo;
                 for (unsigned int c = 0; c < 2u; c++) {
-                    unsigned long long cid =
-                        hrm::mix64(id64 ^ (((unsigned long long)p.step << 1) | c) * 0x9E3779B97F4A7C15ull);
+                    unsigned long long cid = child_id(id64, p.step, c);
                     Photon q = p;
                     q.id_lo = (unsigned int)cid;
                     q.id_hi = (unsigned int)(cid >> 32);
