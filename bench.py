@@ -194,7 +194,7 @@ def flush_l2(buf):
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one exec launch on a
 # small case of the same kernel, with its call count: scaled by calls to the bench's launch
 # (profiles/photon_walk_async_exec_kernel_ncu.txt: 10^5 photons, variant R4/T2).
-TRAFFIC_PROFILE = {("photon", "async"): (2792448 + 1518080, 161486336)}
+TRAFFIC_PROFILE = {("photon", "async"): (2631936 + 375808, 161486336)}
 
 BYTES_PER_CALL = {
     "photon": [93, 92, 48],

@@ -147,16 +147,16 @@ struct PhotonMove {
         if (ty < tb) { tb = ty; axis = 1; }
         if (tz < tb) { tb = tz; axis = 2; }
         p.step += 1u;
-        if (dist < tb) {
-            p.x = hrm::fadd(p.x, hrm::fmul(dist, p.dx));
-            p.y = hrm::fadd(p.y, hrm::fmul(dist, p.dy));
-            p.z = hrm::fadd(p.z, hrm::fmul(dist, p.dz));
+        // Advance to the collision point, or to the face crossed first.
+        const bool collide = dist < tb;
+        const float t = collide ? dist : tb;
+        p.x = hrm::fadd(p.x, hrm::fmul(t, p.dx));
+        p.y = hrm::fadd(p.y, hrm::fmul(t, p.dy));
+        p.z = hrm::fadd(p.z, hrm::fmul(t, p.dz));
+        if (collide) {
             prog.template async<PhotonCollide>(p);
             return;
         }
-        p.x = hrm::fadd(p.x, hrm::fmul(tb, p.dx));
-        p.y = hrm::fadd(p.y, hrm::fmul(tb, p.dy));
-        p.z = hrm::fadd(p.z, hrm::fmul(tb, p.dz));
         // Land exactly on the face and step the voxel index along the crossing axis (written
         // with selects, so that the lanes of a warp crossing different faces do not diverge).
         const float d_axis = axis == 0 ? p.dx : (axis == 1 ? p.dy : p.dz);
