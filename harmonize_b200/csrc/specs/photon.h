@@ -67,25 +67,29 @@ HRM_HD HRM_FI unsigned long long to_fixed(float x) {
     return (unsigned long long)hrm::fmul(x, 4294967296.0f);
 }
 
+// One Marsaglia trial on the random words (a, b): true, with the direction set, if the
+// point (u, v) they give falls inside the unit disc (and is not its centre).
+HRM_HD HRM_FI bool disc_trial(unsigned int a, unsigned int b, float& dx, float& dy, float& dz) {
+    const float u = hrm::u_pm1(a);
+    const float v = hrm::u_pm1(b);
+    const float s = hrm::fadd(hrm::fmul(u, u), hrm::fmul(v, v));
+    if (!(s < 1.0f && s > 0.0f)) return false;
+    const float f = hrm::fmul(2.0f, hrm::fsqrt(hrm::fsub(1.0f, s)));
+    dx = hrm::fmul(u, f);
+    dy = hrm::fmul(v, f);
+    dz = hrm::fsub(1.0f, hrm::fmul(2.0f, s));
+    return true;
+}
+
 // Isotropic unit vector by Marsaglia's method (Ann. Math. Stat. 43, 1972): draw (u, v)
 // uniform in the unit disc, return (2u*sqrt(1-s), 2v*sqrt(1-s), 1-2s) with s = u^2+v^2.
+// Each Philox draw gives two trials, (x, y) then (z, w).
 HRM_HD HRM_FI void isotropic(const PhotonState& st, unsigned int id_lo, unsigned int id_hi, unsigned int step,
                              float& dx, float& dy, float& dz) {
     for (unsigned int a = 0; a < 16u; a++) {
-        hrm::U32x4 r = photon_rng(st, id_lo, id_hi, step, PHASE_DIR + a);
-        unsigned int pair[4] = {r.x, r.y, r.z, r.w};
-        for (unsigned int q = 0; q < 4u; q += 2u) {
-            float u = hrm::u_pm1(pair[q]);
-            float v = hrm::u_pm1(pair[q + 1]);
-            float s = hrm::fadd(hrm::fmul(u, u), hrm::fmul(v, v));
-            if (s < 1.0f && s > 0.0f) {
-                float f = hrm::fmul(2.0f, hrm::fsqrt(hrm::fsub(1.0f, s)));
-                dx = hrm::fmul(u, f);
-                dy = hrm::fmul(v, f);
-                dz = hrm::fsub(1.0f, hrm::fmul(2.0f, s));
-                return;
-            }
-        }
+        const hrm::U32x4 r = photon_rng(st, id_lo, id_hi, step, PHASE_DIR + a);
+        if (disc_trial(r.x, r.y, dx, dy, dz)) return;
+        if (disc_trial(r.z, r.w, dx, dy, dz)) return;
     }
     dx = 0.0f;
     dy = 0.0f;
