@@ -249,10 +249,8 @@ struct Batch : BatchBase {
         unsigned int ctr[8] = {n, 0u, 0u, 0u, closed0, 0u, 0u, 0u};
         ck(cudaMemcpyAsync(jobs.data(), recs.data(), sizeof(JobRecord) * n, cudaMemcpyHostToDevice, stream), "jobs");
         ck(cudaMemcpyAsync(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice, stream), "counters");
-        cudaEvent_t e0, e1;
-        ck(cudaEventCreate(&e0), "event");
-        ck(cudaEventCreate(&e1), "event");
-        ck(cudaEventRecord(e0, stream), "event");
+        hrm_capi::EventPair ev;
+        ck(cudaEventRecord(ev.start, stream), "event");
         ck(cudaGraphLaunch(graph, stream), "graph launch");
         size_t execs = 1;
         ck(cudaStreamSynchronize(stream), "batch exec");
@@ -263,12 +261,8 @@ struct Batch : BatchBase {
             ck(cudaStreamSynchronize(stream), "batch exec");
             done = inst.complete();
         }
-        ck(cudaEventRecord(e1, stream), "event");
-        ck(cudaEventSynchronize(e1), "event");
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        ck(cudaEventRecord(ev.stop, stream), "event");
+        const float ms = ev.elapsed_ms();
         std::vector<JobRecord> out(n);
         unsigned long long start = 0;
         ck(cudaMemcpy(out.data(), jobs.data(), sizeof(JobRecord) * n, cudaMemcpyDeviceToHost), "jobs back");

@@ -175,10 +175,8 @@ int run_to_completion(ProgramBase* p, const hrm_run_config& cfg, hrm_run_result*
     size_t groups = cfg.groups ? cfg.groups : (size_t)1 << 30;
     size_t n = (p->type == HRM_ASYNC) ? (cfg.cycles ? cfg.cycles : ((size_t)1 << 24)) : (cfg.chunk ? cfg.chunk : 1);
     size_t max_execs = cfg.max_execs ? cfg.max_execs : 4096;
-    cudaEvent_t e0, e1;
-    ck(cudaEventCreate(&e0), "cudaEventCreate");
-    ck(cudaEventCreate(&e1), "cudaEventCreate");
-    ck(cudaEventRecord(e0, s), "cudaEventRecord");
+    hrm_capi::EventPair ev;
+    ck(cudaEventRecord(ev.start, s), "cudaEventRecord");
     p->set_tuning(cfg.patience, cfg.fill_links);
     p->init(groups, s);
     ck(cudaGetLastError(), "init launch");
@@ -199,12 +197,8 @@ int run_to_completion(ProgramBase* p, const hrm_run_config& cfg, hrm_run_result*
     } catch (DeviceFlagError& e) {
         status = fail(HRM_EDEVICE, e.what());
     }
-    ck(cudaEventRecord(e1, s), "cudaEventRecord");
-    ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    ck(cudaEventRecord(ev.stop, s), "cudaEventRecord");
+    const float ms = ev.elapsed_ms();
     if (res) {
         res->flags = p->flags();
         res->execs = (uint32_t)execs;
