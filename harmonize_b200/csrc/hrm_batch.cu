@@ -431,6 +431,16 @@ struct Server : ServerBase {
           cycles(cfg.cycles ? cfg.cycles : ((size_t)1 << 20)),
           arena_links(cfg.arena ? cfg.arena : ((size_t)1 << 21)),
           solo_photons(cfg.solo_photons) {
+        try {
+            set_up(cap, cfg);
+        } catch (...) {
+            release_host_resources();  // the destructor does not run for a failed constructor
+            throw;
+        }
+        runner = std::thread([this] { loop(); });
+    }
+
+    void set_up(unsigned int cap, const hrm_run_config& cfg) {
         ck(cudaHostAlloc((void**)&done_host, sizeof(unsigned long long) * cap, cudaHostAllocMapped), "done flags");
         memset(done_host, 0, sizeof(unsigned long long) * cap);
         ck(cudaHostGetDevicePointer((void**)&done_dev, done_host, 0), "done flags device alias");
@@ -459,7 +469,18 @@ struct Server : ServerBase {
         mix_prepare_range_kernel<<<1, 32, 0, submit_s>>>(jobs.data(), 0u, 0u);
         ck(cudaGetLastError(), "kernel load");
         ck(cudaStreamSynchronize(submit_s), "kernel load");
-        runner = std::thread([this] { loop(); });
+    }
+
+    void release_host_resources() {
+        if (exec_s) cudaStreamDestroy(exec_s);
+        if (submit_s) cudaStreamDestroy(submit_s);
+        if (done_host) cudaFreeHost(done_host);
+        if (staging) cudaFreeHost(staging);
+        if (pinned_ctr) cudaFreeHost(pinned_ctr);
+        exec_s = submit_s = nullptr;
+        done_host = nullptr;
+        staging = nullptr;
+        pinned_ctr = nullptr;
     }
 
     // Teardown is bounded: the session is closed, the running exec is asked to halt (teams
@@ -475,11 +496,7 @@ struct Server : ServerBase {
             cudaStreamSynchronize(submit_s);
             runner.join();
         }
-        if (exec_s) cudaStreamDestroy(exec_s);
-        if (submit_s) cudaStreamDestroy(submit_s);
-        if (done_host) cudaFreeHost(done_host);
-        if (staging) cudaFreeHost(staging);
-        if (pinned_ctr) cudaFreeHost(pinned_ctr);
+        release_host_resources();
     }
 
     // Relaunches the persistent kernel until the session is closed and every job is done.
