@@ -72,6 +72,8 @@ struct BfsSpec {
     static const size_t POOL_SIZE = 8191;
     static const size_t RING_LINKS = RING;
     static const size_t TEAMS_PER_CTA = TEAMS;
+    // Relax calls with smaller levels first: fewer vertices are expanded more than once.
+    static const size_t OLDEST_FIRST = 1;
 
     template <typename PROGRAM>
     HRM_DEV static void initialize(PROGRAM) {}

@@ -83,6 +83,7 @@ class AsyncProgram {
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
     static const unsigned int COALESCE_PATIENCE =
         (unsigned int)hrm_rt::spec_COALESCE_PATIENCE<PROGRAM_SPEC>::value;
+    static const bool OLDEST_FIRST = hrm_rt::spec_OLDEST_FIRST<PROGRAM_SPEC>::value != 0;
 
     static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
     static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
@@ -703,16 +704,22 @@ class AsyncProgram {
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         const unsigned int cnt = g.count[F];
+        const unsigned int bottom = g.bottom[F];
         Promise<Op> p;
         if (lane < k) {
             unsigned int w[W];
-            unsigned int slot = (g.bottom[F] + cnt - k + lane) & (SLOTS - 1);
+            // The k newest promises (top of the ring), or the k oldest (bottom) for specs that
+            // ask for OLDEST_FIRST; calls made by the batch are appended at the top either way.
+            unsigned int slot = ((OLDEST_FIRST ? bottom : bottom + cnt - k) + lane) & (SLOTS - 1);
 #pragma unroll
             for (unsigned int i = 0; i < W; i++) w[i] = g.words[BASE + i * SLOTS + slot];
             p.from_words(w);
         }
         __syncwarp();
-        if (lane == 0) g.count[F] = cnt - k;
+        if (lane == 0) {
+            g.count[F] = cnt - k;
+            if (OLDEST_FIRST) g.bottom[F] = (bottom + k) & (SLOTS - 1);
+        }
         __syncwarp();
         if (lane < k) {
             p(*this);
