@@ -5,8 +5,10 @@ one fill takes from the arena) with the highest throughput on the GPU it runs on
 
     python -m harmonize_b200.autotune [--specs photon,bfs,collatz,batched] [--reps 2]
 
-Single-spec workloads are scored by async calls/s; "batched" (a seeded 384-job mix of all
-three specs in one persistent launch, the job-multiplexing spec) by jobs/s.
+Single-spec workloads are scored by async calls/s, except BFS, scored by searches per second
+(its call count depends on the order of evaluation, so fewer calls can be the faster run);
+"batched" (a seeded 384-job mix of all three specs in one persistent launch, the
+job-multiplexing spec) by jobs/s.
 
 Writes harmonize_b200/tuned.json: {"<workload>/<program>": {"variant": v, "ring_links": r,
 "teams_per_cta": t, "patience": p, "fill_links": f, "score": x, "unit": ..., "sweep": [...]}}.
@@ -91,14 +93,15 @@ def tune(specs, reps=2, programs=("async", "event")):
                 try:
                     for _ in range(reps + 1):
                         res = work[spec](prog, **cand)
-                        best = max(best, res["evals"] / (res["device_ms"] / 1e3))
+                        work_done = 1.0 if spec == "bfs" else res["evals"]
+                        best = max(best, work_done / (res["device_ms"] / 1e3))
                 except Exception as e:  # a configuration that fails is not selectable
                     sweep.append(dict(cand, error=str(e)))
                     continue
                 sweep.append(dict(cand, score=best))
             b = _best(sweep)
             if b:
-                _record(table, f"{spec}/{prog}", b, sweep, "calls/s")
+                _record(table, f"{spec}/{prog}", b, sweep, "searches/s" if spec == "bfs" else "calls/s")
     with open(TUNED_PATH, "w") as f:
         json.dump(table, f, indent=1, sort_keys=True)
     return table

@@ -357,6 +357,11 @@ struct MixSpec {
     struct RING_LINKS_OF {
         static const size_t value = RING_GROUP_OF<Op>::value == JOB_PHOTON ? RING : 2 * RING;
     };
+    // BFS jobs take their teams' oldest calls first, as the BFS spec does on its own.
+    template <typename Op>
+    struct OLDEST_FIRST_OF {
+        static const bool value = RING_GROUP_OF<Op>::value == JOB_BFS;
+    };
 
     template <typename PROGRAM>
     HRM_DEV static void initialize(PROGRAM prog) {

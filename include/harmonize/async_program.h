@@ -83,7 +83,6 @@ class AsyncProgram {
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
     static const unsigned int COALESCE_PATIENCE =
         (unsigned int)hrm_rt::spec_COALESCE_PATIENCE<PROGRAM_SPEC>::value;
-    static const bool OLDEST_FIRST = hrm_rt::spec_OLDEST_FIRST<PROGRAM_SPEC>::value != 0;
 
     static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
     static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
@@ -701,6 +700,7 @@ class AsyncProgram {
         constexpr unsigned int W = Promise<Op>::WORDS;
         constexpr unsigned int SLOTS = ring_slots<F>();
         constexpr unsigned int BASE = ring_base<F>();
+        constexpr bool OLDEST_FIRST = hrm_rt::fn_OLDEST_FIRST<PROGRAM_SPEC, Op>::value;
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         const unsigned int cnt = g.count[F];
@@ -708,8 +708,8 @@ class AsyncProgram {
         Promise<Op> p;
         if (lane < k) {
             unsigned int w[W];
-            // The k newest promises (top of the ring), or the k oldest (bottom) for specs that
-            // ask for OLDEST_FIRST; calls made by the batch are appended at the top either way.
+            // The k newest promises (top of the ring), or the k oldest (bottom) for functions
+            // whose spec asks for OLDEST_FIRST; the batch's calls are appended at the top.
             unsigned int slot = ((OLDEST_FIRST ? bottom : bottom + cnt - k) + lane) & (SLOTS - 1);
 #pragma unroll
             for (unsigned int i = 0; i < W; i++) w[i] = g.words[BASE + i * SLOTS + slot];

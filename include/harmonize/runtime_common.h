@@ -83,6 +83,16 @@ template <class S, class Op>
 struct fn_RING_GROUP<S, Op, std::void_t<decltype(S::template RING_GROUP_OF<Op>::value)>>
     : std::integral_constant<unsigned int, (unsigned int)(S::template RING_GROUP_OF<Op>::value)> {};
 
+// Pop order per function: a spec may define
+//   template <typename Op> struct OLDEST_FIRST_OF { static const bool value = ...; };
+// to choose OLDEST_FIRST function by function (e.g. only for the search functions of a spec
+// that multiplexes several programs); otherwise every function follows OLDEST_FIRST.
+template <class S, class Op, class = void>
+struct fn_OLDEST_FIRST : std::integral_constant<bool, spec_OLDEST_FIRST<S>::value != 0> {};
+template <class S, class Op>
+struct fn_OLDEST_FIRST<S, Op, std::void_t<decltype(S::template OLDEST_FIRST_OF<Op>::value)>>
+    : std::integral_constant<bool, (bool)(S::template OLDEST_FIRST_OF<Op>::value)> {};
+
 template <class S, class P, class = void>
 struct has_initialize : std::false_type {};
 template <class S, class P>
