@@ -8,6 +8,7 @@
    clear_flags / destroy, the counterparts of the generated alloc_program_S, init_program_S,
    exec_program_S, complete_S, clear_flags_S and free_program_S of harmonize/python/templates.py),
    with small exec budgets so that a run spans many execs and resumes from the queues it left.
+3. Failure detection without a fault: the runtime's bounded waits, made to run out on purpose.
 """
 import os
 import struct
@@ -79,3 +80,18 @@ def test_c_abi_life_cycle(hrm, program, groups, n):
         assert prog.flags() == 0
     finally:
         prog.close()
+
+
+@pytest.mark.gpu
+def test_waits_that_nobody_ends_time_out_with_a_status(tmp_path):
+    """tests/cpp/wait_timeouts.cu makes each bounded wait of the runtime run out on purpose (a
+    queue entry never published, a full queue nobody drains, a grid barrier one CTA short):
+    each raises WAIT_TIMEOUT and returns an error instead of spinning, the context stays
+    usable, and a normal publish-and-take round trip raises nothing."""
+    exe = tmp_path / "wait_timeouts"
+    subprocess.run(["nvcc", "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "wait_timeouts.cu"),
+                    "-o", str(exe)], check=True, capture_output=True, timeout=600)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count("timed out as expected") == 3 and "no wait ran out" in r.stdout
