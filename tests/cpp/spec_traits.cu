@@ -1,0 +1,45 @@
+// Compile-time checks of the optional spec members this runtime reads (no kernel runs): a
+// member a spec defines is honoured, a member it leaves out takes its default, and the
+// per-function forms (RING_LINKS_OF, RING_GROUP_OF, OLDEST_FIRST_OF) override the spec-wide
+// ones function by function. Built with `nvcc -c`; a failed check is a compile error.
+#include "harmonize.h"
+#include "../../harmonize_b200/csrc/specs/mix.h"
+
+using namespace hrm_specs;
+using hrm_rt::fn_OLDEST_FIRST;
+using hrm_rt::fn_RING_GROUP;
+using hrm_rt::fn_RING_LINKS;
+
+// Spec-wide values, and their defaults.
+static_assert(hrm_rt::spec_RING_LINKS<PhotonSpec<4, 2>>::value == 4, "RING_LINKS from the spec");
+static_assert(hrm_rt::spec_TEAMS_PER_CTA<PhotonSpec<4, 2>>::value == 2, "TEAMS_PER_CTA from the spec");
+static_assert(hrm_rt::spec_MIN_CTAS_PER_SM<PhotonSpec<4, 2>>::value == 1, "MIN_CTAS_PER_SM default");
+static_assert(hrm_rt::spec_COALESCE_PATIENCE<CollatzSpec<>>::value == 16, "COALESCE_PATIENCE default");
+static_assert(hrm_rt::spec_OLDEST_FIRST<CollatzSpec<>>::value == 0, "OLDEST_FIRST default");
+static_assert(hrm_rt::spec_OLDEST_FIRST<BfsSpec<>>::value == 1, "BFS takes oldest first");
+
+// Per function, single-spec: every function follows the spec-wide value.
+static_assert(fn_OLDEST_FIRST<BfsSpec<2, 8>, BfsRelax>::value && fn_OLDEST_FIRST<BfsSpec<2, 8>, BfsExpand>::value,
+              "BFS functions oldest first");
+static_assert(!fn_OLDEST_FIRST<PhotonSpec<4, 2>, PhotonMove>::value, "photon newest first");
+static_assert(!fn_OLDEST_FIRST<CollatzSpec<>, CollatzOdd>::value, "Collatz newest first");
+static_assert(fn_RING_LINKS<PhotonSpec<4, 2>, PhotonTally>::value == 4, "no RING_LINKS_OF: RING_LINKS");
+static_assert(fn_RING_GROUP<PhotonSpec<4, 2>, PhotonMove>::value == 0, "no RING_GROUP_OF: one group");
+
+// Per function, the job-multiplexing spec: groups by job kind, photon rings RING links and
+// the others 2*RING, BFS functions oldest first and the others newest first.
+using Mix42 = MixSpec<4, 2>;
+static_assert(fn_RING_GROUP<Mix42, Job<CollatzEven>>::value == JOB_COLLATZ, "Collatz group");
+static_assert(fn_RING_GROUP<Mix42, Job<PhotonCollide>>::value == JOB_PHOTON, "photon group");
+static_assert(fn_RING_GROUP<Mix42, Job<BfsExpand>>::value == JOB_BFS, "BFS group");
+static_assert(fn_RING_LINKS<Mix42, Job<PhotonMove>>::value == 4, "photon rings");
+static_assert(fn_RING_LINKS<Mix42, Job<CollatzEven>>::value == 8, "Collatz rings");
+static_assert(fn_RING_LINKS<Mix42, Job<BfsRelax>>::value == 8, "BFS rings");
+static_assert(fn_OLDEST_FIRST<Mix42, Job<BfsRelax>>::value && fn_OLDEST_FIRST<Mix42, Job<BfsExpand>>::value,
+              "BFS jobs oldest first");
+static_assert(!fn_OLDEST_FIRST<Mix42, Job<PhotonMove>>::value && !fn_OLDEST_FIRST<Mix42, Job<CollatzEven>>::value,
+              "other jobs newest first");
+
+// Discriminants are 0-based positions in the OpUnion, as in the original runtime.
+static_assert(OpUnionLookup<PhotonTally, PhotonSpec<4, 2>::OpSet>::DISC == 2, "DISC = position");
+static_assert(OpUnionLookup<Job<BfsExpand>, Mix42::OpSet>::DISC == 6, "DISC = position");

@@ -41,6 +41,17 @@ def test_header_compiles_as_c():
     assert r.returncode == 0, r.stderr
 
 
+def test_spec_members_are_honoured_at_compile_time(tmp_path):
+    """tests/cpp/spec_traits.cu: static checks that optional spec members (ring sizes, teams,
+    patience, pop order, ring groups, and their per-function forms) reach the runtime and that
+    omitted ones take their defaults. nvcc cross-compiles it here; no kernel runs."""
+    src = os.path.join(ROOT, "tests", "cpp", "spec_traits.cu")
+    r = subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I", os.path.join(ROOT, "include"), "-c", src, "-o", str(tmp_path / "traits.o")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 def test_bad_arguments_return_einval(hrm):
     L = hrm.lib()
     res = hrm.RunResult()
