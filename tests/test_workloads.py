@@ -1,0 +1,30 @@
+"""CPU checks that the seeded synthetic job mix has the shapes and distributions of the batched
+and serving workload: 4096 instances in equal thirds; Collatz ranges of lognormal length
+(median 2^12, sigma 1.5) clipped to [2^6, 2^20]; photon batches of 10^3..10^6 photons,
+log-uniform; BFS on R-MAT graphs of 2^12..2^18 vertices."""
+import numpy as np
+
+from harmonize_b200 import jobs
+
+
+def test_job_mix_shapes_and_distributions():
+    specs = jobs.make_mix_specs(4096, seed=1)
+    kinds = np.array([s["kind"] for s in specs])
+    assert [int((kinds == k).sum()) for k in (jobs.JOB_COLLATZ, jobs.JOB_PHOTON, jobs.JOB_BFS)] == [1366, 1365, 1365]
+    lengths = np.array([s["count"] for s in specs if s["kind"] == jobs.JOB_COLLATZ])
+    assert lengths.min() >= 64 and lengths.max() <= 1 << 20
+    assert abs(np.median(np.log2(lengths)) - 12) < 0.2
+    inner = np.log(lengths[(lengths > 64) & (lengths < 1 << 20)])
+    assert abs(inner.std() - 1.5) < 0.15  # clipping trims the tails a little
+    photons = np.array([s["count"] for s in specs if s["kind"] == jobs.JOB_PHOTON])
+    assert photons.min() >= 1000 and photons.max() <= 1_000_000
+    exps = np.log10(photons)
+    assert abs(np.median(exps) - 4.5) < 0.15 and abs(exps.mean() - 4.5) < 0.1
+    scales = np.array([s["scale"] for s in specs if s["kind"] == jobs.JOB_BFS])
+    assert scales.min() == 12 and scales.max() == 18
+    assert all(0 <= s["root"] < 1 << s["scale"] for s in specs if s["kind"] == jobs.JOB_BFS)
+
+
+def test_job_mix_is_seeded():
+    assert jobs.make_mix_specs(300, seed=5) == jobs.make_mix_specs(300, seed=5)
+    assert jobs.make_mix_specs(300, seed=5) != jobs.make_mix_specs(300, seed=6)
