@@ -28,3 +28,17 @@ def test_job_mix_shapes_and_distributions():
 def test_job_mix_is_seeded():
     assert jobs.make_mix_specs(300, seed=5) == jobs.make_mix_specs(300, seed=5)
     assert jobs.make_mix_specs(300, seed=5) != jobs.make_mix_specs(300, seed=6)
+
+
+def test_rmat_graph_shape():
+    """R-MAT (a, b, c) = (0.57, 0.19, 0.19): E = 16 * V directed edges, and the skew of the
+    recursion puts a heavy share of them on low vertex ids (vertex 0 expects E * (a+b)^scale)."""
+    import harmonize_b200 as hrm
+    scale = 14
+    rp, col = hrm.rmat_csr(scale, 16, 0.57, 0.19, 0.19, 3)
+    deg = np.diff(rp.astype(np.int64))
+    assert len(col) == 16 << scale and deg.sum() == len(col)
+    assert col.max() < 1 << scale
+    expected0 = (16 << scale) * (0.57 + 0.19) ** scale
+    assert 0.5 * expected0 < deg[0] < 2.0 * expected0
+    assert deg.max() > 100 * deg.mean()  # heavy-tailed: far above the mean degree of 16
