@@ -529,37 +529,35 @@ class AsyncProgram {
     // -----------------------------------------------------------------------------------
     static const unsigned int NULL_LINK = 0xFFFFFFFFu;
 
-    // The lanes of `mask` (all calling with promises of TYPE) store their promises into one
-    // fresh arena link, in rank order. Returns the link to every lane, or NULL_LINK if the
+    // One lane: a fresh arena link with its written-count word cleared, or NULL_LINK if the
     // arena is exhausted (ARENA_EXHAUSTED_FLAG raised).
+    __device__ unsigned int alloc_held_link() {
+        unsigned int link = NULL_LINK;
+        const unsigned int got = alloc_links_coop(1, 0, 1u << util::lane_id(), link);
+        if (got == 0 || link == NULL_LINK) {
+            hrm_rt::raise_flag(_dev_ctx.ctl, hrm_rt::ARENA_EXHAUSTED_FLAG);
+            return NULL_LINK;
+        }
+        _dev_ctx.link_meta[2u * link + 1u] = 0u;
+        return link;
+    }
+    // One lane: returns an unused link to the free ring.
+    __device__ void free_held_link(unsigned int link) { free_links_coop(link, 0, 1, 1u << util::lane_id()); }
+
+    // Stores promise p into slot `slot` (< 32) of arena link `link`.
     template <typename TYPE>
-    __device__ unsigned int hold_in_link(const Promise<TYPE>& p, unsigned int mask) {
+    __device__ __forceinline__ void store_in_link(const Promise<TYPE>& p, unsigned int link, unsigned int slot) {
         constexpr unsigned int W = Promise<TYPE>::WORDS;
         unsigned int w[W];
         p.to_words(w);
-        const unsigned int r = __popc(mask & util::lanemask_lt());
-        const unsigned int leader = __ffs(mask) - 1;
-        unsigned int link = NULL_LINK;
-        unsigned int got = alloc_links_coop(1, r, mask, link);
-        link = __shfl_sync(mask, link, leader);
-        if (got == 0 || link == NULL_LINK) {
-            if (r == 0) hrm_rt::raise_flag(_dev_ctx.ctl, hrm_rt::ARENA_EXHAUSTED_FLAG);
-            return NULL_LINK;
-        }
 #pragma unroll
-        for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, r), w[i]);
-        if (r == 0) {
-            _dev_ctx.link_meta[2u * link + 0u] = 0u;
-            _dev_ctx.link_meta[2u * link + 1u] = (unsigned int)__popc(mask);
-        }
-        __threadfence();
-        __syncwarp(mask);
-        return link;
+        for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, slot), w[i]);
     }
 
+    // Per held link: `next` word (the barrier's stack) and the number of promises written.
     __device__ __forceinline__ unsigned int* link_next_ptr(unsigned int link) { return &_dev_ctx.link_meta[2u * link]; }
-    __device__ __forceinline__ unsigned int link_count(unsigned int link) {
-        return hrm_rt::ld_relaxed(&_dev_ctx.link_meta[2u * link + 1u]);
+    __device__ __forceinline__ unsigned int* link_written_ptr(unsigned int link) {
+        return &_dev_ctx.link_meta[2u * link + 1u];
     }
 
     // One lane: publishes a held link of function f to its queue.

@@ -42,3 +42,15 @@ def test_barrier_demo_rejects_event_program_and_zero_barriers(hrm):
         hrm.barrier_demo(10, 1, 2, program="event")
     with pytest.raises(hrm.HarmonizeError):
         hrm.barrier_demo(10, 1, 0)
+
+
+@pytest.mark.gpu
+def test_held_promises_of_different_warps_share_links(hrm):
+    """2^20 held follow-ups spread over 1000 barriers: the lanes of one warp all await different
+    barriers, so one link per warp group would take 2^20 arena links. Packed into each
+    barrier's partial link across warps they need about 2^15 (+ one partial per barrier), so
+    an arena of 2^16 links is enough and the run is exact."""
+    dep, ndep, bar = 1 << 20, 1 << 10, 1000
+    counter, released, _ = hrm.barrier_demo(dep, ndep, bar, arena=1 << 16)
+    assert counter.tolist() == [2 * dep + ndep + 1, ndep, 1, 0]
+    assert released[:bar].tolist() == [dep // bar + (1 if dep % bar > b else 0) for b in range(bar)]
