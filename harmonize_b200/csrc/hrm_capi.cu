@@ -13,6 +13,7 @@
 
 #include <chrono>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -250,15 +251,17 @@ struct Staging {
     }
 };
 std::mutex g_staging_mutex;
-std::map<int, std::unique_ptr<Staging>> g_staging;
+std::map<int, std::shared_ptr<Staging>> g_staging;
 
-Staging& staging() {
+// Shared ownership: hrm_release_cache drops the map's reference, and a run in progress keeps
+// its staging alive until it ends.
+std::shared_ptr<Staging> staging() {
     int dev = 0;
     ck(cudaGetDevice(&dev), "cudaGetDevice");
     std::lock_guard<std::mutex> lock(g_staging_mutex);
     auto& s = g_staging[dev];
-    if (!s) s.reset(new Staging());
-    return *s;
+    if (!s) s = std::make_shared<Staging>();
+    return s;
 }
 
 // Program instances of the whole-run helpers, kept per (device, spec, type, variant,
@@ -271,20 +274,22 @@ struct CacheKey {
     }
 };
 std::mutex g_cache_mutex;
-std::map<CacheKey, std::unique_ptr<ProgramBase>> g_cache;
+std::map<CacheKey, std::shared_ptr<ProgramBase>> g_cache;
 
+// Shared ownership, as for staging: a run holds its instance until it ends, even if
+// hrm_release_cache drops the cache's reference meanwhile.
 template <typename STATE>
-ProgramBase* cached_program(int spec, int type, int variant, size_t arena, const STATE& st) {
+std::shared_ptr<ProgramBase> cached_program(int spec, int type, int variant, size_t arena, const STATE& st) {
     int dev = 0;
     ck(cudaGetDevice(&dev), "cudaGetDevice");
     CacheKey key{dev, spec, type, variant, arena};
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     auto it = g_cache.find(key);
     if (it == g_cache.end()) {
-        it = g_cache.emplace(key, std::unique_ptr<ProgramBase>(make_program(spec, type, arena, &st, sizeof(st),
+        it = g_cache.emplace(key, std::shared_ptr<ProgramBase>(make_program(spec, type, arena, &st, sizeof(st),
                                                                             variant))).first;
     }
-    return it->second.get();
+    return it->second;
 }
 
 hrm_run_config config_or_default(const hrm_run_config* cfg) {
@@ -305,13 +310,13 @@ int collatz_run(uint32_t start, uint32_t count, uint32_t* d_out, const hrm_run_c
     st.iterator = nullptr;
     st.leap = 1;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_COLLATZ, cfg.program_type);
-    ProgramBase* p = cached_program(HRM_SPEC_COLLATZ, cfg.program_type, cfg.variant, arena, st);
+    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_COLLATZ, cfg.program_type, cfg.variant, arena, st);
     std::lock_guard<std::mutex> run(p->run_lock);
     util::iter::AtomicIter<unsigned int> host_it(start, start + count);
     ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     st.iterator = p->iterator.data();
     p->set_state(&st, sizeof(st));
-    return run_to_completion(p, cfg, res);
+    return run_to_completion(p.get(), cfg, res);
 }
 
 // Photon walk with device-resident medium and tally (tally zeroed here).
@@ -337,13 +342,13 @@ int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32
     // splits grow a batch of photons several-fold before roulette thins it.
     st.load_limit = 0.015625f;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_PHOTON, cfg.program_type);
-    ProgramBase* p = cached_program(HRM_SPEC_PHOTON, cfg.program_type, cfg.variant, arena, st);
+    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_PHOTON, cfg.program_type, cfg.variant, arena, st);
     std::lock_guard<std::mutex> run(p->run_lock);
     util::iter::AtomicIter<unsigned int> host_it(first, first + count);
     ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     st.source = p->iterator.data();
     p->set_state(&st, sizeof(st));
-    return run_to_completion(p, cfg, res);
+    return run_to_completion(p.get(), cfg, res);
 }
 
 // BFS over a device-resident CSR graph; levels initialised here.
@@ -361,13 +366,13 @@ int bfs_run(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t nv, uint32
     st.root = root;
     st.nv = nv;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_BFS, cfg.program_type);
-    ProgramBase* p = cached_program(HRM_SPEC_BFS, cfg.program_type, cfg.variant, arena, st);
+    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_BFS, cfg.program_type, cfg.variant, arena, st);
     std::lock_guard<std::mutex> run(p->run_lock);
     util::iter::AtomicIter<unsigned int> host_it(0, 1);
     ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     st.roots = p->iterator.data();
     p->set_state(&st, sizeof(st));
-    return run_to_completion(p, cfg, res);
+    return run_to_completion(p.get(), cfg, res);
 }
 
 // Remapping-barrier workload; counters and barriers are set up here, results copied out.
@@ -402,13 +407,13 @@ int barrier_demo_run(uint32_t dep, uint32_t ndep, uint32_t bar, uint32_t* counte
     st.barriers = dbars.ptr;
     st.unit = dunit.ptr;
     size_t arena = cfg.arena ? cfg.arena : ((size_t)1 << 18);
-    ProgramBase* p = cached_program(HRM_SPEC_BARRIER_DEMO, HRM_ASYNC, cfg.variant, arena, st);
+    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_BARRIER_DEMO, HRM_ASYNC, cfg.variant, arena, st);
     std::lock_guard<std::mutex> run(p->run_lock);
     util::iter::AtomicIter<unsigned int> host_it(0, dep + ndep);
     ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     st.source = p->iterator.data();
     p->set_state(&st, sizeof(st));
-    int rc = run_to_completion(p, cfg, res);
+    int rc = run_to_completion(p.get(), cfg, res);
     if (rc != HRM_OK) return rc;
     ck(cudaMemcpyAsync(counter, dcount.ptr, 16, cudaMemcpyDeviceToHost, s), "counter download");
     ck(cudaMemcpyAsync(released, drel.ptr, (size_t)bar * 4u, cudaMemcpyDeviceToHost, s), "counter download");
@@ -566,7 +571,8 @@ int hrm_collatz_run(uint32_t start, uint32_t count, uint32_t* out, const hrm_run
     HRM_GUARD({
         hrm_run_config cfg = config_or_default(cfg_in);
         cudaStream_t s = (cudaStream_t)cfg.stream;
-        Staging& st = staging();
+        std::shared_ptr<Staging> st_ref = staging();
+        Staging& st = *st_ref;
         std::lock_guard<std::mutex> staged(st.lock);
         uint32_t* d = st.get<uint32_t>(0, count);
         int rc = collatz_run(start, count, d, &cfg, res);
@@ -594,7 +600,8 @@ int hrm_photon_run(const float* mu_s, const float* absorb, const uint8_t* split,
         cudaStream_t s = (cudaStream_t)cfg.stream;
         const size_t nvox = (size_t)n * n * n;
         const size_t slots = nvox + 3u * hrm_specs::PHOTON_SPREAD;
-        Staging& st = staging();
+        std::shared_ptr<Staging> st_ref = staging();
+        Staging& st = *st_ref;
         std::lock_guard<std::mutex> staged(st.lock);
         float* dm = st.get<float>(0, nvox);
         float* da = st.get<float>(1, nvox);
@@ -625,7 +632,8 @@ int hrm_bfs_run(const uint32_t* rowptr, const uint32_t* col, uint32_t nv, uint32
         hrm_run_config cfg = config_or_default(cfg_in);
         cudaStream_t s = (cudaStream_t)cfg.stream;
         const size_t ne = rowptr[nv];
-        Staging& st = staging();
+        std::shared_ptr<Staging> st_ref = staging();
+        Staging& st = *st_ref;
         std::lock_guard<std::mutex> staged(st.lock);
         uint32_t* drp = st.get<uint32_t>(0, (size_t)nv + 1);
         uint32_t* dcol = st.get<uint32_t>(1, ne ? ne : 1);

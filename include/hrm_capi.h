@@ -118,7 +118,7 @@ int hrm_device_sync(void);
  * device memory; concurrent runs on the same cached instance are serialised. The host-buffer
  * runs (hrm_collatz_run, hrm_photon_run, hrm_bfs_run) likewise keep their device copies of
  * inputs and outputs per device, grown on demand, and run one at a time per device. This
- * frees both. */
+ * frees both; what a run in progress on another thread uses is freed when that run ends. */
 int hrm_release_cache(void);
 
 /* ---- program life cycle (templates.py:3-184 counterparts) ------------------------------

@@ -55,3 +55,25 @@ def test_every_compiled_variant_matches_oracle(hrm, medium16, variant):
         rp, col = hrm.rmat_csr(12, 8, seed=5)
         levels, _ = hrm.bfs(rp, col, 0, program=program, variant=variant)
         assert np.array_equal(levels, oracle.bfs(rp, col, 0))
+
+
+@pytest.mark.gpu
+def test_release_cache_while_another_thread_runs(hrm):
+    """hrm_release_cache drops the cached instances and staging buffers; a whole run in
+    progress on another thread keeps what it uses until it ends, and its result is exact."""
+    import threading
+    import time
+
+    mu, ab, sp = hrm.photon_medium(64, 5)
+    got = {}
+
+    def run():
+        got["tally"] = hrm.photon_walk(mu, ab, sp, 64, 17, 0, 200000)[0]
+
+    t = threading.Thread(target=run)
+    t.start()
+    time.sleep(0.003)
+    hrm.check(hrm.lib().hrm_release_cache())
+    t.join()
+    again = hrm.photon_walk(mu, ab, sp, 64, 17, 0, 200000)[0]
+    assert np.array_equal(got["tally"], again)
