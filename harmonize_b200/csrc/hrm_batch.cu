@@ -401,7 +401,8 @@ struct Server : ServerBase {
     unsigned long long* done_host = nullptr;    // mapped: %globaltimer of completion per job
     JobRecord* staging = nullptr;               // pinned staging for job records
     unsigned int* pinned_ctr = nullptr;         // pinned staging for counter writes
-    unsigned int capacity, submitted = 0;
+    unsigned int capacity;
+    std::atomic<unsigned int> submitted{0};  // written by submit, read by poll and close
     size_t groups, cycles;
     cudaStream_t exec_s = nullptr, submit_s = nullptr;
     std::thread runner;
@@ -409,6 +410,7 @@ struct Server : ServerBase {
     std::atomic<bool> stop{false};
     std::mutex err_lock;
     std::string err;
+    std::mutex submit_lock;
     size_t arena_links;
     // Solo lane: photon jobs of at least solo_photons photons fill the GPU on their own and run
     // at about half speed inside the multiplexing kernel, so the session serves them alone
@@ -557,6 +559,7 @@ struct Server : ServerBase {
     }
 
     unsigned int submit(const hrm_job* in, unsigned int n) override {
+        std::lock_guard<std::mutex> one_at_a_time(submit_lock);  // submissions from several threads
         if (submitted + n > capacity) throw std::invalid_argument("server job table is full");
         unsigned int first = submitted;
         std::vector<std::pair<unsigned int, hrm_job>> solo;
@@ -601,7 +604,7 @@ struct Server : ServerBase {
 
     unsigned int poll(uint64_t* done_ns, unsigned int max) override {
         unsigned int c = 0;
-        unsigned int m = std::min(max, submitted);
+        unsigned int m = std::min(max, submitted.load());
         for (unsigned int j = 0; j < m; j++) {
             unsigned long long t = ((volatile unsigned long long*)done_host)[j];
             if (done_ns) done_ns[j] = t;
@@ -616,7 +619,8 @@ struct Server : ServerBase {
         ck(cudaMemcpyAsync(counters.data() + 2, pinned_ctr + 1, 4, cudaMemcpyHostToDevice, submit_s), "close");
         ck(cudaStreamSynchronize(submit_s), "close");
         auto t0 = std::chrono::steady_clock::now();
-        while (poll(nullptr, submitted) < submitted) {
+        const unsigned int total = submitted.load();
+        while (poll(nullptr, total) < total) {
             if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms)) {
                 throw std::runtime_error("serving session did not finish within the close timeout");
             }
@@ -631,8 +635,9 @@ struct Server : ServerBase {
 
     // Device-side state of up to 8 unfinished jobs, for error messages.
     std::string describe_unfinished() override {
-        std::vector<JobRecord> recs(submitted);
-        if (submitted == 0 || cudaMemcpy(recs.data(), jobs.data(), sizeof(JobRecord) * submitted,
+        const unsigned int total = submitted.load();
+        std::vector<JobRecord> recs(total);
+        if (total == 0 || cudaMemcpy(recs.data(), jobs.data(), sizeof(JobRecord) * total,
                                          cudaMemcpyDeviceToHost) != cudaSuccess)
             return "";
         unsigned int ctr[8] = {};
@@ -641,7 +646,7 @@ struct Server : ServerBase {
                         std::to_string(ctr[4]) + " low " + std::to_string(ctr[5]) + " flags " +
                         std::to_string(inst.flags()) + "]";
         int shown = 0;
-        for (unsigned int j = 0; j < submitted && shown < 8; j++) {
+        for (unsigned int j = 0; j < total && shown < 8; j++) {
             const JobRecord& r = recs[j];
             if (r.done) continue;
             s += " job " + std::to_string(j) + ": kind " + std::to_string(r.kind) + " pending " +
