@@ -1,0 +1,48 @@
+"""CPU checks of bench.py's reporting helpers: the clock record taken during the timed region
+(median SM clock, max clock, throttle reasons), the latency percentiles, the algorithmic
+bytes behind the roofline, and the measured HBM peak it is divided by."""
+import json
+import os
+
+import numpy as np
+
+import bench
+
+
+def test_clock_summary_reads_clocks_and_throttle_reasons():
+    s = bench.ClockSampler(0)
+    s.lines = [
+        "0, 1965, 1965, 700.5, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1950, 1965, 990.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1965, 1965, 800.0, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "garbage line",
+    ]
+    out = s.summary()
+    assert out == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    s.lines = ["0, 1200, 1965, 500, 0x8, Active, Not Active, Active, Not Active"]
+    assert s.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+    s.lines = []
+    assert s.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def test_latency_percentiles_in_ms():
+    ns = np.arange(1, 1001) * 1_000_000  # 1 .. 1000 ms
+    p = bench.percentiles_ms(ns)
+    assert p["max"] == 1000.0 and abs(p["p50"] - 500.5) < 1e-9
+    assert abs(p["p99"] - np.percentile(np.arange(1, 1001), 99)) < 1e-9
+    assert p["p50"] <= p["p99"] <= p["p99.9"] <= p["max"]
+
+
+def test_algorithmic_bytes_weight_each_function_by_its_bytes():
+    stats = {"fn0_evals": 10, "fn1_evals": 5, "fn2_evals": 2}
+    assert bench.algorithmic_bytes(stats, bench.BYTES_PER_CALL["photon"]) == 10 * 93 + 5 * 92 + 2 * 48
+    assert bench.algorithmic_bytes({}, [32, 32]) == 0
+
+
+def test_peak_comes_from_the_measured_file():
+    p = bench.peaks()
+    path = os.path.join(bench.ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        assert p["source"] == "measured" and p["hbm_gbs"] == float(json.load(open(path))["hbm_gbs"])
+    else:
+        assert p["source"] == "fallback"
