@@ -42,3 +42,13 @@ def test_rmat_graph_shape():
     expected0 = (16 << scale) * (0.57 + 0.19) ** scale
     assert 0.5 * expected0 < deg[0] < 2.0 * expected0
     assert deg.max() > 100 * deg.mean()  # heavy-tailed: far above the mean degree of 16
+
+
+def test_poisson_arrivals_have_the_requested_rate():
+    """Serving arrivals: a seeded Poisson process, non-decreasing, mean gap 1/rate."""
+    a = jobs.poisson_arrivals(20000, rate_per_s=500.0, seed=3)
+    gaps = np.diff(np.concatenate([[0], a.astype(np.float64)]))
+    assert np.all(gaps >= 0)
+    assert abs(gaps.mean() / 1e9 - 1 / 500.0) < 0.03 / 500.0
+    assert abs(gaps.std() / gaps.mean() - 1.0) < 0.05  # exponential gaps: std = mean
+    assert np.array_equal(a, jobs.poisson_arrivals(20000, rate_per_s=500.0, seed=3))
