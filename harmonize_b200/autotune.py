@@ -30,10 +30,11 @@ BATCH_VARIANTS = (0, 1, 2)  # the variants the job-multiplexing spec is built fo
 
 
 def load_tuned():
+    """The tuned table, or {} when none was written (a damaged file raises)."""
     try:
         with open(TUNED_PATH) as f:
             return json.load(f)
-    except Exception:
+    except FileNotFoundError:
         return {}
 
 
