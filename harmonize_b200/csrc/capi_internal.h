@@ -44,6 +44,17 @@ struct EventPair {
     }
 };
 
+// Runs `fn` on every path out of the scope that holds the returned object.
+template <typename F>
+struct ScopeExit {
+    F fn;
+    ~ScopeExit() { fn(); }
+};
+template <typename F>
+ScopeExit<F> on_scope_exit(F fn) {
+    return ScopeExit<F>{fn};
+}
+
 template <typename P>
 struct is_async_program : std::false_type {};
 template <typename S>

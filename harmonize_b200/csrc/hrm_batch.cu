@@ -807,15 +807,23 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
             srv->close(60000);
         } else {
             if (nstreams == 0) nstreams = 16;
-            std::vector<cudaStream_t> streams(nstreams);
+            std::vector<cudaStream_t> streams(nstreams, nullptr);
+            std::vector<cudaEvent_t> ev(njobs, nullptr);
+            unsigned int* d_ovf = nullptr;
+            unsigned int* d_fr = nullptr;
+            auto release = hrm_capi::on_scope_exit([&] {  // also when a launch or the deadline throws
+                for (auto& s : streams)
+                    if (s) cudaStreamDestroy(s);
+                for (auto& e : ev)
+                    if (e) cudaEventDestroy(e);
+                if (d_ovf) cudaFree(d_ovf);
+                if (d_fr) cudaFree(d_fr);
+            });
             for (auto& s : streams) ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
-            std::vector<cudaEvent_t> ev(njobs);
             for (auto& e : ev) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
             size_t max_nv = 0;
             for (uint32_t j = 0; j < njobs; j++)
                 if (jobs[j].kind == HRM_JOB_BFS && jobs[j].n > max_nv) max_nv = jobs[j].n;
-            unsigned int* d_ovf = nullptr;
-            unsigned int* d_fr = nullptr;
             ck(cudaMalloc((void**)&d_ovf, 4), "overflow flag");
             ck(cudaMemset(d_ovf, 0, 4), "overflow flag");
             if (max_nv) ck(cudaMalloc((void**)&d_fr, max_nv * 2 * 4 * nstreams), "frontiers");
@@ -872,10 +880,6 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
                 }
             }
             if (makespan_ms) *makespan_ms = (float)(ns_since(t0) / 1e6);
-            for (auto& s : streams) cudaStreamDestroy(s);
-            for (auto& e : ev) cudaEventDestroy(e);
-            cudaFree(d_ovf);
-            if (d_fr) cudaFree(d_fr);
         }
         return HRM_OK;
     } catch (std::invalid_argument& e) {
