@@ -68,6 +68,32 @@ def test_bad_arguments_return_einval(hrm):
     assert L.hrm_program_complete(None, None) == hrm.HRM_EINVAL
 
 
+def test_job_and_input_entry_points_reject_bad_arguments(hrm):
+    """The batch, serving and input entry points check their arguments before any CUDA call."""
+    L = hrm.lib()
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    out = vp()
+    assert L.hrm_server_open(u32(0), None, ctypes.byref(out)) == hrm.HRM_EINVAL       # zero capacity
+    assert L.hrm_server_open(u32(4), None, None) == hrm.HRM_EINVAL                    # no handle
+    first = u32()
+    assert L.hrm_server_submit(None, None, u32(0), ctypes.byref(first)) == hrm.HRM_EINVAL
+    assert L.hrm_server_poll(None, None, u32(0), None) == hrm.HRM_EINVAL
+    assert L.hrm_server_close(None, u32(10)) == hrm.HRM_EINVAL
+    assert L.hrm_server_destroy(None) == hrm.HRM_OK                                   # like free(NULL)
+    assert L.hrm_batch_run(None, u32(3), None, None, None) == hrm.HRM_EINVAL
+    assert L.hrm_plain_run(None, u32(3), u32(4), None, None) == hrm.HRM_EINVAL
+    assert L.hrm_runtime_run(None, u32(3), 0, None, None, None) == hrm.HRM_EINVAL
+    assert L.hrm_serve_replay(None, u32(3), None, 0, u32(1), None, None, None) == hrm.HRM_EINVAL
+    rp = np.zeros(5, dtype=np.uint32)
+    col = np.zeros(16, dtype=np.uint32)
+    assert L.hrm_rmat_csr(2, 4, ctypes.c_double(0.6), ctypes.c_double(0.3), ctypes.c_double(0.3), ctypes.c_uint64(1),
+                          rp.ctypes.data, col.ctypes.data) == 1                       # a + b + c > 1
+    assert L.hrm_rmat_csr(0, 4, ctypes.c_double(0.5), ctypes.c_double(0.2), ctypes.c_double(0.2), ctypes.c_uint64(1),
+                          rp.ctypes.data, col.ctypes.data) == 1                       # scale 0
+    mu = np.zeros(8, dtype=np.float32)
+    assert L.hrm_photon_medium(0, ctypes.c_uint64(1), mu.ctypes.data, mu.ctypes.data, None) == 1
+
+
 def test_product_fails_loudly_without_its_library(monkeypatch, tmp_path):
     import harmonize_b200 as h
     monkeypatch.setattr(h, "_lib", None)
