@@ -16,7 +16,11 @@ e2e   : the same metric through the host-buffer entry point (hrm_*_run): input u
 exchange), photon ids offset per rank (weak scaling); time = max over ranks.
 --impl reference: the reference runtime (Harmonize's own runtime built from its headers with
 the same spec source into oracle/_ref: its EventProgram for the photon walk, on which its
-AsyncProgram faulted) on the same workload and metric, over a bounded sample per step.
+AsyncProgram faulted, at the launch shape its sweep found best) on the same workload, config
+and metric; that process loads only oracle/ libraries.
+After the timed steps, rank 0 checks the last run's output against the CPU oracle over the
+whole workload ("oracle_check": "exact", or the bench fails); that oracle run (OpenMP host
+executor of the same spec source) is the line's cpu_baseline.
 --workload batched / serving: the job mix in the persistent runtime against one single-spec
 runtime run per job and one plain kernel per job (see run_batched / run_serving).
 """
@@ -177,6 +181,21 @@ def replica_range(rank, count):
     return rank * count, count
 
 
+def workload_config(args, world):
+    """The workload of the bench line, shared by both arms (the reference arm reports the same
+    dict): what is run, not how."""
+    l2 = "flushed before every step (256 MiB write)"
+    if args.workload == "photon":
+        return {"workload": f"photon_walk_{args.photons:.0e}_photons_{args.grid}^3", "photons_per_gpu": args.photons,
+                "grid": args.grid, "l2": l2,
+                "medium": "seeded synthetic: mu_s~lognormal(0,0.5), absorb~U[0.02,0.2], split p=0.1 (seed 2024)",
+                "parallelism": f"replicas x{world}"}
+    if args.workload == "bfs":
+        return {"workload": f"rmat_bfs_2^{args.scale}_ef16", "vertices": 1 << args.scale,
+                "edges": 16 << args.scale, "root": 0, "l2": l2, "parallelism": f"replicas x{world}"}
+    return {"workload": "collatz_1_to_2^20", "starts": 1 << 20, "l2": l2, "parallelism": f"replicas x{world}"}
+
+
 def flush_l2(buf):
     buf.zero_()  # 256 MiB > the 126 MB L2
 
@@ -241,26 +260,22 @@ def run_photon(args, hrm, rank, world, pg, torch):
                  - int(t[nvox + 2048:].sum()))
         return int(t.sum(dtype=np.uint64)), total / 2.0 ** 32
 
-    def cpu_sample(target_s=10.0):
+    def oracle_check():
+        """The whole workload on the OpenMP host executor of the same spec source, compared bit
+        for bit with the last timed run's tallies; its time is the CPU baseline."""
         import oracle
         threads = oracle.max_threads()
-        k = 2000
+        got = d_tally.cpu().numpy().view(np.uint64)
         t0 = time.perf_counter()
-        _, calls = oracle.exec_photon(mu, ab, sp, n, seed, first, k, threads=threads)
+        ref, calls = oracle.exec_photon(mu, ab, sp, n, seed, first, count, threads=threads)
         dt = time.perf_counter() - t0
-        k2 = int(min(2_000_000, max(k, k * target_s / max(dt, 1e-3))))
-        t0 = time.perf_counter()
-        _, calls = oracle.exec_photon(mu, ab, sp, n, seed, first, k2, threads=threads)
-        dt = time.perf_counter() - t0
-        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
-                "sample": f"{k2} photons of the same 128^3 medium, OpenMP host executor of the same spec source, "
-                          f"{int(calls.sum())} calls in {dt:.2f} s"}
+        cpu = {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+               "sample": f"the whole workload ({count} photons on the {n}^3 medium), OpenMP host executor of the "
+                         f"same spec source, {int(calls.sum())} calls in {dt:.1f} s"}
+        return np.array_equal(got, ref), cpu
 
-    config = {"workload": f"photon_walk_{count:.0e}_photons_{n}^3", "photons_per_gpu": count, "grid": n,
-              "program": args.program, "l2": "flushed before every step (256 MiB write)",
-              "medium": "seeded synthetic: mu_s~lognormal(0,0.5), absorb~U[0.02,0.2], split p=0.1"}
-    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
-                config=config, h2d=int(mu.nbytes + ab.nbytes + sp.nbytes), d2h=int(slots * 8), dtype="f32",
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
+                h2d=int(mu.nbytes + ab.nbytes + sp.nbytes), d2h=int(slots * 8), dtype="f32",
                 bytes_per_call=BYTES_PER_CALL["photon"], launches_per_step=3 if args.program == "async" else 2)
 
 
@@ -293,19 +308,20 @@ def run_bfs(args, hrm, rank, world, pg, torch):
         lv = d_lev.cpu().numpy().view(np.uint32)
         return int(lv.astype(np.uint64).sum()), int((lv != 0xFFFFFFFF).sum())
 
-    def cpu_sample(target_s=10.0):
+    def oracle_check():
         import oracle
         threads = oracle.max_threads()
+        got = d_lev.cpu().numpy().view(np.uint32)
+        ok = np.array_equal(got, oracle.bfs(rp, col, 0))
         t0 = time.perf_counter()
         _, calls = oracle.exec_bfs(rp, col, 0, threads=threads)
         dt = time.perf_counter() - t0
-        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
-                "sample": f"full R-MAT 2^{args.scale} BFS, OpenMP host executor of the same spec source"}
+        cpu = {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+               "sample": f"full R-MAT 2^{args.scale} BFS, OpenMP host executor of the same spec source"}
+        return ok, cpu
 
-    config = {"workload": f"rmat_bfs_2^{args.scale}_ef16", "vertices": nv, "edges": int(len(col)),
-              "program": args.program, "l2": "flushed before every step (256 MiB write)"}
-    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
-                config=config, h2d=int(rp.nbytes + col.nbytes), d2h=int(nv * 4), dtype="u32",
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
+                h2d=int(rp.nbytes + col.nbytes), d2h=int(nv * 4), dtype="u32",
                 bytes_per_call=BYTES_PER_CALL["bfs"], launches_per_step=3 if args.program == "async" else 2)
 
 
@@ -332,19 +348,20 @@ def run_collatz(args, hrm, rank, world, pg, torch):
         o = d_out.cpu().numpy().view(np.uint32)
         return int(o.astype(np.uint64).sum()), int(o.max())
 
-    def cpu_sample(target_s=10.0):
+    def oracle_check():
         import oracle
         threads = oracle.max_threads()
+        got = d_out.cpu().numpy().view(np.uint32)
+        ok = np.array_equal(got, oracle.collatz_range(start, count))
         t0 = time.perf_counter()
         _, calls = oracle.exec_collatz(start, count, threads=threads)
         dt = time.perf_counter() - t0
-        return {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
-                "sample": "n = 1..2^20, OpenMP host executor of the same spec source"}
+        cpu = {"value": float(calls.sum()) / dt, "unit": "calls/s", "cores": threads, "kind": "port",
+               "sample": "n = 1..2^20, OpenMP host executor of the same spec source"}
+        return ok, cpu
 
-    config = {"workload": "collatz_1_to_2^20", "starts": count, "program": args.program,
-              "l2": "flushed before every step (256 MiB write)"}
-    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, cpu_sample=cpu_sample,
-                config=config, h2d=0, d2h=count * 4, dtype="u64",
+    return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
+                h2d=0, d2h=count * 4, dtype="u64",
                 bytes_per_call=BYTES_PER_CALL["collatz"], launches_per_step=3 if args.program == "async" else 2)
 
 
@@ -468,7 +485,7 @@ def main():
     args = parse()
     if args.impl == "reference":
         from oracle import reference_bench
-        return reference_bench.main(args)
+        return reference_bench.main(args, workload_config(args, int(os.environ.get("WORLD_SIZE", "1"))))
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "serving":
@@ -540,12 +557,16 @@ def main():
                 "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes = each call's promise written and read once plus its compulsory "
                         "application bytes; the launch duration is the whole run (init + exec kernels)"}
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        try:
-            cpu = wl["cpu_sample"]()
-        except Exception as e:  # the CPU leg is a reported baseline only
-            cpu = {"value": None, "error": str(e)}
+    # Parity of the timed workload: rank 0 checks its last device-resident run against the
+    # oracle (outside the timed region); the run of the oracle is also the CPU baseline.
+    cpu, oracle_check = None, None
+    if rank == 0 and not args.no_cpu:
+        ok, cpu = wl["oracle_check"]()
+        if not ok:
+            raise SystemExit("bench: the timed run's output differs from the oracle")
+        oracle_check = "exact"
+        if world > 1:
+            cpu = None
     if rank == 0:
         full = s0.get("full_batches", 0) / max(1, s0.get("batches", 1))
         line = {
@@ -553,9 +574,11 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
             "data": "synthetic",
-            "config": dict(wl["config"], parallelism=f"replicas x{world}",
-                           variant=dict(pick_config(args), ring_links_teams_per_cta=list(
-                               hrm.VARIANTS[pick_variant(args, hrm)]))),
+            "config": workload_config(args, world),
+            "implementation": {"program": args.program,
+                               "variant": dict(pick_config(args), ring_links_teams_per_cta=list(
+                                   hrm.VARIANTS[pick_variant(args, hrm)]))},
+            "oracle_check": oracle_check,
             "e2e": {"value": round(e2e_value, 1), "unit": "calls/s", "h2d_bytes_per_step": wl["h2d"],
                     "d2h_bytes_per_step": wl["d2h"]},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),

@@ -442,6 +442,9 @@ int hrm_capi::set_error(int code, const std::string& msg) { return fail(code, ms
         return fail(HRM_ECUDA, e.what());                        \
     }
 
+// Forgets the kept device addresses of the no-allocation scratch area (defined below).
+void noalloc_forget_addresses();
+
 extern "C" {
 
 const char* hrm_last_error(void) { return g_last_error.c_str(); }
@@ -456,6 +459,7 @@ int hrm_device_sync(void) {
 
 int hrm_release_cache(void) {
     HRM_GUARD({
+        noalloc_forget_addresses();
         {
             std::lock_guard<std::mutex> lock(g_cache_mutex);
             g_cache.clear();
@@ -660,9 +664,8 @@ int hrm_barrier_demo_run(uint32_t dep_count, uint32_t non_dep_count, uint32_t ba
 // hrm_collatz_run_device_noalloc: a Collatz whole run that allocates no device memory.
 //
 // Why it exists: some callers cannot call cudaMalloc at the moment they want to run the
-// program. Examples: code recording work into a CUDA stream capture that must not gain
-// allocation nodes, plug-in hosts that hand out only buffers registered ahead of time,
-// and services that forbid allocation after start-up to keep their memory use fixed. Every
+// program. Examples: plug-in hosts that hand out only buffers registered ahead of time, and
+// services that forbid allocation after start-up to keep their memory use fixed. Every
 // other entry point here builds a program instance with cudaMalloc (arena, queues, control
 // block); this one runs the same AsyncProgram<CollatzSpec<2,4>> kernels over a scratch
 // area compiled into the library.
@@ -676,7 +679,10 @@ int hrm_barrier_demo_run(uint32_t dep_count, uint32_t non_dep_count, uint32_t ba
 // a kernel handed it would fault or, where the GPU can reach host memory, silently use the
 // wrong memory. So the first call on each device, with that device current, looks up the
 // device address once with cudaGetSymbolAddress and keeps it; make that first call before
-// any stream capture starts.
+// any stream capture starts. A device reset unloads the module and so invalidates the kept
+// address: hrm_release_cache() forgets it, and the next call looks it up again. The run
+// itself waits on the host for each exec (it reads the flags back to decide whether to
+// launch another) and reads the statistics back with a synchronous copy at the end.
 //
 // All calls share the one array, which keeps the previous call's contents; each call
 // rewrites everything the run needs initialised. Calls that overlap on the GPU (several host
@@ -722,6 +728,15 @@ unsigned char* noalloc_scratch_address() {
     }
     return g_na_address[dev];
 }
+
+}  // namespace
+
+void noalloc_forget_addresses() {
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    for (auto& a : g_na_address) a = nullptr;
+}
+
+namespace {
 
 // Sets the start-value iterator that lives in the scratch area.
 __global__ void noalloc_iterator_kernel(util::iter::AtomicIter<unsigned int>* it, unsigned int start,

@@ -291,9 +291,9 @@ int hrm_serve_replay_runtime(const hrm_job* jobs, uint32_t njobs, const uint64_t
 
 /* ---- run without device allocation ------------------------------------------------------
  * No counterpart in the original Harmonize (every original program instance allocates its
- * buffers). For callers that cannot call cudaMalloc when they run a program: code recording
- * into a CUDA stream capture that must not gain allocation nodes, plug-in hosts that only
- * hand out buffers registered ahead of time, services that fix their memory use at start-up.
+ * buffers). For callers that cannot call cudaMalloc when they run a program: plug-in hosts
+ * that only hand out buffers registered ahead of time, and services that forbid allocation
+ * after start-up to keep their memory use fixed.
  * Same result as hrm_collatz_run_device with AsyncProgram and variant 0, but the runtime's
  * arena, queues and control block live in a scratch area compiled into the library (about
  * 2.2 MiB, held on every GPU that loads the library until the process exits). The caller
@@ -301,9 +301,13 @@ int hrm_serve_replay_runtime(const hrm_job* jobs, uint32_t njobs, const uint64_t
  * HRM_NOALLOC_MAX_ARENA_LINKS (0 means that maximum; larger is rejected with HRM_EINVAL), and
  * a run whose promises in flight outgrow it stops with HRM_EDEVICE (ARENA_EXHAUSTED);
  * program_type must be HRM_ASYNC and variant 0. The first call on each device looks up the
- * scratch area's device address (cudaGetSymbolAddress), so make it before any stream capture.
- * All calls share the scratch area and each call re-initialises it; calls that overlap on
- * the GPU race, so serialise them. res->device_ms is host wall time for this entry point. */
+ * scratch area's device address (cudaGetSymbolAddress) and keeps it, so make that first call
+ * before any stream capture begins; after cudaDeviceReset on a device, call
+ * hrm_release_cache() before the next call so that the address is looked up again. The call
+ * waits for every exec it launches (it reads the device flags back after each one), and reads
+ * the statistics back before it returns. All calls share the scratch area and each call
+ * re-initialises it; calls that overlap on the GPU race, so serialise them. res->device_ms is
+ * host wall time for this entry point. */
 #define HRM_NOALLOC_MAX_ARENA_LINKS 4096
 int hrm_collatz_run_device_noalloc(uint32_t start, uint32_t count, uint32_t* d_out_steps,
                                    const hrm_run_config* cfg, hrm_run_result* res);

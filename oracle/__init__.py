@@ -18,5 +18,5 @@ reference runtime's own outputs (``tests/golden``); the photon and BFS restateme
 bit for bit with the host executors of the spec sources and with the reference runtime.
 """
 from .lib import (load, max_threads, collatz_range, exec_collatz, bfs, exec_bfs,  # noqa: F401
-                  photon_walk, exec_photon, philox, log, PHOTON_SPREAD,
+                  photon_walk, exec_photon, photon_medium, rmat_csr, philox, log, PHOTON_SPREAD,
                   ref_load, ref_collatz, ref_photon_device, ref_bfs_device, REF_WG, REF_CYCLES)

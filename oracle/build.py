@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
 
-C_SOURCES = ["collatz.c", "bfs.c", "photon.c"]
+C_SOURCES = ["collatz.c", "bfs.c", "photon.c", "inputs.c"]
 CXX_SOURCES = ["host_exec.cpp"]
 SPEC_DIR = os.path.join(HERE, "..", "harmonize_b200", "csrc", "specs")
 
@@ -43,7 +43,7 @@ def build(force=False, quiet=True):
         subprocess.run(cmd, check=True, capture_output=quiet)
         objs.append(o)
     tmp = LIB + ".tmp"
-    subprocess.run(["g++", "-shared", "-fopenmp", "-o", tmp] + objs, check=True, capture_output=quiet)
+    subprocess.run(["g++", "-shared", "-fopenmp", "-o", tmp] + objs + ["-lm"], check=True, capture_output=quiet)
     os.replace(tmp, LIB)
     return LIB
 

@@ -27,6 +27,8 @@ def load():
             "oracle_exec_collatz": (None, [u32, u32, vp, i32, vp]),
             "oracle_exec_photon": (None, [vp, vp, vp, u32, u32, u32, u32, u32, vp, i32, vp]),
             "oracle_exec_bfs": (None, [vp, vp, u32, u32, vp, i32, vp]),
+            "oracle_photon_medium": (i32, [u32, u64, vp, vp, vp]),
+            "oracle_rmat_csr": (i32, [u32, u32, ctypes.c_double, ctypes.c_double, ctypes.c_double, u64, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -84,6 +86,29 @@ def _medium_args(mu_s, absorb, split):
     return mu_s, absorb, split
 
 
+def photon_medium(n, seed):
+    """Seeded n^3 photon medium (mu_s float32, absorb float32, split uint8), restated here so
+    that oracle-side callers need not load the product library."""
+    nv = n ** 3
+    mu = np.empty(nv, dtype=np.float32)
+    ab = np.empty(nv, dtype=np.float32)
+    sp = np.empty(nv, dtype=np.uint8)
+    if load().oracle_photon_medium(n, seed, mu.ctypes.data, ab.ctypes.data, sp.ctypes.data) != 0:
+        raise ValueError("bad medium arguments")
+    return mu, ab, sp
+
+
+def rmat_csr(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1):
+    """Seeded R-MAT graph as CSR (rowptr uint32[2^scale+1], col uint32[E]), restated here so
+    that oracle-side callers need not load the product library."""
+    nv = 1 << scale
+    rowptr = np.empty(nv + 1, dtype=np.uint32)
+    col = np.empty(edge_factor * nv, dtype=np.uint32)
+    if load().oracle_rmat_csr(scale, edge_factor, a, b, c, seed, rowptr.ctypes.data, col.ctypes.data) != 0:
+        raise ValueError("bad R-MAT arguments")
+    return rowptr, col
+
+
 def photon_walk(mu_s, absorb, split, n, seed, first, count):
     """Plain-C restatement of the photon walk. Returns (tally uint64[n^3+3*1024], calls[3])."""
     mu_s, absorb, split = _medium_args(mu_s, absorb, split)
@@ -138,7 +163,8 @@ def ref_load():
         L.ref_collatz_run.restype = i32
         L.ref_collatz_run.argtypes = [i32, u32, u32, vp, u32, u32, u32, u32, fp, up]
         L.ref_photon_run_device.restype = i32
-        L.ref_photon_run_device.argtypes = [i32, vp, vp, vp, u32, u64, u32, u32, vp, u32, u32, u32, u32, fp, up]
+        L.ref_photon_run_device.argtypes = [i32, vp, vp, vp, u32, u64, u32, u32, vp, u32, u32, u32, u32,
+                                            ctypes.c_float, fp, up]
         L.ref_bfs_run_device.restype = i32
         L.ref_bfs_run_device.argtypes = [i32, vp, vp, u32, u32, vp, u32, u32, u32, u32, fp, up]
         _ref = L
@@ -168,29 +194,42 @@ def ref_collatz(start, count, program="async", wg=REF_WG, n=None, arena=None, ma
 
 
 # The reference AsyncProgram raised an illegal memory access on the photon spec (record in
-# profiles/reference_asyncprogram_photon_fault.txt); it is suspected for every spec whose evals
-# make several async calls, so those specs run only on the reference EventProgram.
-REF_ASYNC_CLOSED = "reference AsyncProgram faulted (illegal memory access) on multi-call specs; not run again"
+# profiles/reference_asyncprogram_photon_fault.txt). Reading its code found defects that any
+# spec whose evals make several async calls from divergent lanes can reach (unsynchronised stash
+# updates by two lane groups of one warp, a spilled partial link left in the partial map, empty
+# stash slots and arena links used without a check for none); none is proven to be the cause,
+# so the photon spec stays on the reference EventProgram and BFS, whose Expand evals make many
+# calls from divergent lanes, is not run on the reference AsyncProgram either. Collatz runs on it.
+REF_ASYNC_CLOSED_PHOTON = "reference AsyncProgram faulted (illegal memory access) on the photon spec; not run again"
+REF_ASYNC_CLOSED_BFS = ("reference AsyncProgram not run on BFS: its Expand evals reach the defects read in the "
+                        "reference AsyncProgram (divergent multi-call stash updates)")
+
+# Launch shape of the reference EventProgram on the photon walk: the best of the sweep in
+# profiles/reference_eventprogram_photon_sweep.txt (oracle/ref_sweep.py).
+REF_PHOTON_SHAPE = {"wg": REF_WG, "chunk": 1, "io": 1 << 24, "load_limit": 1.0 / 64}
 
 
-def ref_photon_device(d_mu, d_ab, d_sp, n, seed, first, count, d_tally, program="event", wg=REF_WG, nn=None,
-                      arena=None, max_execs=200000):
-    """Pointers are device addresses (ints). Returns timing dict; tally left in d_tally."""
+def ref_photon_device(d_mu, d_ab, d_sp, n, seed, first, count, d_tally, program="event", wg=None, nn=None,
+                      arena=None, max_execs=200000, load_limit=None):
+    """Pointers are device addresses (ints). Returns timing dict; tally left in d_tally.
+    Defaults: REF_PHOTON_SHAPE."""
     if program != "event":
-        raise RuntimeError(REF_ASYNC_CLOSED)
+        raise RuntimeError(REF_ASYNC_CLOSED_PHOTON)
     pt = 1
-    nn = nn if nn is not None else (REF_CYCLES if pt == 0 else 1)
-    arena = arena if arena is not None else ((1 << 20) if pt == 0 else (1 << 24))
+    wg = wg if wg is not None else REF_PHOTON_SHAPE["wg"]
+    nn = nn if nn is not None else REF_PHOTON_SHAPE["chunk"]
+    arena = arena if arena is not None else REF_PHOTON_SHAPE["io"]
+    load_limit = load_limit if load_limit is not None else REF_PHOTON_SHAPE["load_limit"]
     ms, ex = ctypes.c_float(), ctypes.c_uint32()
     _ref_check(ref_load().ref_photon_run_device(pt, d_mu, d_ab, d_sp, n, seed, first, count, d_tally, wg, nn, arena,
-                                                max_execs, ctypes.byref(ms), ctypes.byref(ex)))
+                                                max_execs, load_limit, ctypes.byref(ms), ctypes.byref(ex)))
     return {"ms": ms.value, "execs": ex.value}
 
 
 def ref_bfs_device(d_rowptr, d_col, nv, root, d_levels, program="event", wg=REF_WG, nn=None, arena=None,
                    max_execs=200000):
     if program != "event":
-        raise RuntimeError(REF_ASYNC_CLOSED)
+        raise RuntimeError(REF_ASYNC_CLOSED_BFS)
     pt = 1
     nn = nn if nn is not None else (REF_CYCLES if pt == 0 else 1)
     arena = arena if arena is not None else ((1 << 20) if pt == 0 else (1 << 24))

@@ -114,10 +114,11 @@ int ref_collatz_run(int program_type, uint32_t start, uint32_t count, uint32_t* 
     }
 }
 
-// Photon walk: medium already on the device (device-resident timing); tally out to host.
+// Photon walk: medium already on the device (device-resident timing); tally left in d_tally.
 int ref_photon_run_device(int program_type, const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32_t n,
                           uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally, uint32_t wg_count,
-                          uint32_t nn, uint32_t arena, uint32_t max_execs, float* ms, uint32_t* execs) {
+                          uint32_t nn, uint32_t arena, uint32_t max_execs, float load_limit, float* ms,
+                          uint32_t* execs) {
     try {
         const size_t slots = (size_t)n * n * n + 3u * hrm_specs::PHOTON_SPREAD;
         ck(cudaMemset(d_tally, 0, slots * 8u), "tally");
@@ -134,7 +135,9 @@ int ref_photon_run_device(int program_type, const float* d_mu, const float* d_ab
         st.seed_lo = (uint32_t)seed;
         st.seed_hi = (uint32_t)(seed >> 32);
         st.leap = 1;
-        st.load_limit = 0.015625f;
+        // EventProgram: make_work stops launching photons while the move buffer is fuller than
+        // this fraction (0 selects 1/64).
+        st.load_limit = load_limit > 0.0f ? load_limit : 0.015625f;
         return drive_spec<hrm_specs::PhotonSpec>(program_type, arena, st, wg_count, nn, max_execs, ms, execs);
     } catch (std::exception& e) {
         g_ref_error = e.what();

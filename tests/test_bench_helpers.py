@@ -46,3 +46,28 @@ def test_peak_comes_from_the_measured_file():
         assert p["source"] == "measured" and p["hbm_gbs"] == float(json.load(open(path))["hbm_gbs"])
     else:
         assert p["source"] == "fallback"
+
+
+def _args(**kw):
+    import argparse
+    d = dict(workload="photon", photons=10_000_000, grid=128, scale=22, program="async", variant=-1)
+    d.update(kw)
+    return argparse.Namespace(**d)
+
+
+def test_both_arms_report_the_same_workload_config():
+    """The config names the workload only; how it is run (program type, tuning variant, the
+    reference's launch shape) is reported beside it, so both arms print equal configs."""
+    for wl in ("photon", "bfs", "collatz"):
+        a = bench.workload_config(_args(workload=wl, program="async"), 1)
+        b = bench.workload_config(_args(workload=wl, program="event", variant=3), 1)
+        assert a == b and "program" not in a and "variant" not in a
+    assert bench.workload_config(_args(), 1)["workload"] == "photon_walk_1e+07_photons_128^3"
+
+
+def test_reference_side_scripts_do_not_load_the_product():
+    """The reference arm, the reference sweep and the golden-fixture script build their inputs
+    with the oracle's own generators, so their processes map no library of the product."""
+    for rel in ("oracle/reference_bench.py", "oracle/ref_sweep.py", "tests/golden/make_golden.py"):
+        src = open(os.path.join(bench.ROOT, rel)).read()
+        assert "harmonize_b200" not in src, rel

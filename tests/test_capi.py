@@ -137,3 +137,36 @@ def test_ctypes_structs_match_the_c_layout(hrm, tmp_path):
     assert got[1] == [C.job_order.offset, C.solo_photons.offset]
     assert got[2] == [ctypes.sizeof(hrm.RunResult), hrm.RunResult.device_ms.offset]
     assert got[3] == [ctypes.sizeof(jobs.Job), jobs.Job.out.offset]
+
+
+def _noalloc(hrm):
+    f = hrm.lib().hrm_collatz_run_device_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.POINTER(hrm.RunConfig),
+                  ctypes.POINTER(hrm.RunResult)]
+    return f
+
+
+@pytest.mark.parametrize("cfg_kw,message", [
+    (dict(program="async", arena=4097), "exceeds the no-allocation maximum"),
+    (dict(program="event"), "AsyncProgram only"),
+    (dict(program="async", variant=2), "tuning variant 0 only"),
+])
+def test_noalloc_rejects_bad_configs_before_any_cuda_call(hrm, cfg_kw, message):
+    """The no-allocation entry point checks its arguments before it touches the device: an
+    arena beyond HRM_NOALLOC_MAX_ARENA_LINKS, EventProgram and other variants are refused with
+    HRM_EINVAL. The output pointer is a dummy that is never dereferenced."""
+    f = _noalloc(hrm)
+    cfg = hrm.make_config(**cfg_kw)
+    res = hrm.RunResult()
+    rc = f(0, 16, ctypes.c_void_p(0x1000), ctypes.byref(cfg), ctypes.byref(res))
+    assert rc == hrm.HRM_EINVAL
+    assert message in hrm.lib().hrm_last_error().decode()
+
+
+def test_noalloc_rejects_null_output_and_overflowing_range(hrm):
+    f = _noalloc(hrm)
+    cfg = hrm.make_config("async")
+    res = hrm.RunResult()
+    assert f(0, 16, None, ctypes.byref(cfg), ctypes.byref(res)) == hrm.HRM_EINVAL
+    assert f(0xFFFFFFF0, 0x20, ctypes.c_void_p(0x1000), ctypes.byref(cfg), ctypes.byref(res)) == hrm.HRM_EINVAL

@@ -119,3 +119,33 @@ def test_barrier_oracle_counts():
         assert counter == [2 * dep + ndep + (1 if ndep else 0), ndep, 1 if ndep else 0, 0]
         assert released == [dep // bar + (1 if dep % bar > b else 0) for b in range(bar)]
         assert sum(released) == dep
+
+
+@pytest.mark.parametrize("n,seed", [(16, 11), (32, 7), (128, 2024)])
+def test_oracle_medium_equals_product_medium(hrm, n, seed):
+    """The oracle's restated medium generator gives the same bytes as the product's
+    hrm_photon_medium (the reference arm and the golden script use the oracle's, so that they
+    never load the product library)."""
+    a = oracle.photon_medium(n, seed)
+    b = hrm.photon_medium(n, seed)
+    for x, y in zip(a, b):
+        assert x.dtype == y.dtype and np.array_equal(x.view(np.uint8), y.view(np.uint8))
+
+
+def test_golden_medium_fixture_is_the_seeded_medium():
+    mu, ab, sp = _medium16()
+    gm, ga, gs = oracle.photon_medium(16, 11)
+    assert np.array_equal(mu, gm) and np.array_equal(ab, ga) and np.array_equal(sp, gs)
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(10, 16, 5), (16, 16, 1), (12, 8, 5)])
+def test_oracle_rmat_equals_product_rmat(hrm, scale, ef, seed):
+    a = oracle.rmat_csr(scale, ef, seed=seed)
+    b = hrm.rmat_csr(scale, ef, seed=seed)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_golden_rmat_fixture_is_the_seeded_graph():
+    g = np.load(os.path.join(GOLDEN, "ref_bfs_rmat10.npz"))
+    rp, col = oracle.rmat_csr(10, 16, seed=5)
+    assert np.array_equal(g["rowptr"], rp) and np.array_equal(g["col"], col)

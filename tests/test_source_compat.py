@@ -12,7 +12,7 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+REF = os.environ.get("HRM_REFERENCE_DIR", "/root/reference")  # overridable reference location
 HEADER = os.path.join(ROOT, "include", "harmonize.h")
 
 EXAMPLES = [
