@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhrm.so")
 SOURCES = [os.path.join(HERE, "csrc", "hrm_capi.cu"), os.path.join(HERE, "csrc", "hrm_batch.cu"),
-           os.path.join(HERE, "csrc", "inputs.cpp")]
+           os.path.join(HERE, "csrc", "inputs.cpp"), os.path.join(HERE, "csrc", "hrm_pyshim.cpp")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "-shared",
@@ -24,7 +24,7 @@ def _deps():
     out = list(SOURCES)
     for d in (os.path.join(ROOT, "include"), os.path.join(HERE, "csrc")):
         for dirpath, _, files in os.walk(d):
-            out += [os.path.join(dirpath, f) for f in files if f.endswith((".h", ".cuh", ".cu"))]
+            out += [os.path.join(dirpath, f) for f in files if f.endswith((".h", ".cuh", ".cu", ".cpp"))]
     return out
 
 

@@ -501,6 +501,14 @@ int hrm_program_destroy(hrm_program* prog) {
     })
 }
 
+int hrm_program_set_state(hrm_program* prog, const void* device_state, size_t state_size) {
+    if (prog == nullptr || device_state == nullptr) return fail(HRM_EINVAL, "program or state is NULL");
+    HRM_GUARD({
+        prog->impl->set_state(device_state, state_size);
+        return HRM_OK;
+    })
+}
+
 int hrm_program_init(hrm_program* prog, size_t groups, void* stream) {
     if (prog == nullptr) return fail(HRM_EINVAL, "program is NULL");
     HRM_GUARD({

@@ -9,6 +9,12 @@
 //    calls (so high-degree vertices spread over many lanes); shorter ranges call Relax once
 //    per edge whose target currently holds a level above l (one async call per edge
 //    relaxation; the read is a filter only, atomicMin decides).
+//    On the GPU the lanes of a batch that evaluate Expand together walk their short ranges
+//    as one flattened edge list: lane L takes edge L, L+k, ... of the concatenation (k =
+//    lanes in the batch), so the col reads of a warp are consecutive addresses and the
+//    level reads of 32 edges are in flight at once, instead of each lane walking its own
+//    range with one dependent load after another. The calls made are the same as lane by
+//    lane (one Relax per edge whose target level is above l when read).
 #ifndef HRM_SPECS_BFS_H
 #define HRM_SPECS_BFS_H
 
@@ -35,12 +41,31 @@ struct BfsExpand {
     using Type = void (*)(unsigned int, unsigned int, unsigned int);
     template <typename PROGRAM>
     HRM_DEV static void eval(PROGRAM prog, unsigned int level, unsigned int begin, unsigned int end) {
+#if defined(__CUDA_ARCH__)
+        // The runtimes evaluate a batch as `if (lane < k) eval(...)`: the active lanes are
+        // 0 .. k-1, which the flattened walk below relies on; any other lane set walks lane
+        // by lane.
+        const unsigned int mask = __activemask();
+        const bool split = end - begin > BFS_CHUNK;
+        if (split) {
+            unsigned int mid = begin + (end - begin) / 2u;
+            prog.template async<BfsExpand>(level, begin, mid);
+            prog.template async<BfsExpand>(level, mid, end);
+        }
+        __syncwarp(mask);
+        if ((mask & (mask + 1u)) == 0u) {
+            expand_flat(prog, mask, level, begin, split ? 0u : end - begin);
+            return;
+        }
+        if (split) return;
+#else
         if (end - begin > BFS_CHUNK) {
             unsigned int mid = begin + (end - begin) / 2u;
             prog.template async<BfsExpand>(level, begin, mid);
             prog.template async<BfsExpand>(level, mid, end);
             return;
         }
+#endif
         for (unsigned int e = begin; e < end; e++) {
             unsigned int u = prog.device.col[e];
             if (hrm::load_relaxed_u32(&prog.device.levels[u]) > level) {
@@ -48,6 +73,49 @@ struct BfsExpand {
             }
         }
     }
+
+#if defined(__CUDA_ARCH__)
+    // Lanes 0 .. k-1 (mask = 2^k - 1) each hold a range of `len` edges from `begin` at
+    // `level`; together they relax the concatenation of the ranges, k edges per round.
+    template <typename PROGRAM>
+    HRM_DEV static void expand_flat(PROGRAM prog, unsigned int mask, unsigned int level, unsigned int begin,
+                                    unsigned int len) {
+        const unsigned int lane = threadIdx.x & 31u;
+        const unsigned int k = 32u - __clz(mask);
+        // Inclusive prefix sum of the range lengths over lanes 0 .. k-1.
+        unsigned int incl = len;
+#pragma unroll
+        for (unsigned int d = 1; d < 32u; d <<= 1) {
+            unsigned int up = __shfl_up_sync(mask, incl, d);
+            if (lane >= d) incl += up;
+        }
+        const unsigned int total = __shfl_sync(mask, incl, k - 1u);
+        for (unsigned int base = 0; base < total; base += k) {
+            const unsigned int p = base + lane;
+            // Owner of edge p: the first lane whose inclusive sum exceeds p (binary search
+            // over lanes 0 .. k-1; every probe reads a lane of the batch).
+            unsigned int lo = 0, hi = k - 1u;
+#pragma unroll
+            for (unsigned int step = 0; step < 5u; step++) {
+                unsigned int mid = (lo + hi) >> 1;
+                unsigned int v = __shfl_sync(mask, incl, mid);
+                if (v > p) hi = mid;
+                else lo = (mid + 1u < hi) ? mid + 1u : hi;
+            }
+            const unsigned int o_incl = __shfl_sync(mask, incl, lo);
+            const unsigned int o_len = __shfl_sync(mask, len, lo);
+            const unsigned int o_begin = __shfl_sync(mask, begin, lo);
+            const unsigned int o_level = __shfl_sync(mask, level, lo);
+            if (p < total) {
+                const unsigned int e = o_begin + (p - (o_incl - o_len));
+                const unsigned int u = prog.device.col[e];
+                if (hrm::load_relaxed_u32(&prog.device.levels[u]) > o_level) {
+                    prog.template async<BfsRelax>(u, o_level);
+                }
+            }
+        }
+    }
+#endif
 };
 
 struct BfsRelax {

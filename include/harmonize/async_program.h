@@ -199,6 +199,7 @@ class AsyncProgram {
         unsigned int bottom[FN];   // ring index of the oldest promise per function
         unsigned int active;       // ring group whose promises the stash holds, or NO_GROUP
         unsigned int held_n;       // overflow links written and not yet published
+        unsigned int loads_pending;  // a lane issued cp.async copies of LazyLoad arguments
         unsigned int held_e[HELD_MAX];  // their queue entries
         unsigned int held_f[HELD_MAX];  // their functions
         unsigned int words[RING_WORDS];
@@ -330,9 +331,20 @@ class AsyncProgram {
     // ===================================================================================
     // Public device API used by specs.
     // ===================================================================================
+    // An argument given as LazyLoad<T>(ref) (promise.h:208-240 of the original, its
+    // ASYNC_LOADS form) is not read at the call: each lane whose promise lands in the team's
+    // shared-memory ring starts an asynchronous copy (cp.async, 4 bytes per argument word)
+    // from `ref` straight into the promise's slot, and the team waits for its copies only
+    // when it next reads its rings (to run or spill a batch), so the load overlaps the rest
+    // of the current batch. A promise that overflows to the arena reads the value at the call.
+    // The referenced memory must not change until the promise first runs.
     template <typename TYPE, typename... ARGS>
     __device__ __forceinline__ void async(ARGS... args) {
-        push_promise<TYPE>(Promise<TYPE>(args...));
+        if constexpr ((hrm_rt::is_lazy_load<ARGS>::value || ...)) {
+            push_lazy<TYPE>(args...);
+        } else {
+            push_promise<TYPE>(Promise<TYPE>(args...));
+        }
     }
     template <typename TYPE>
     __device__ __forceinline__ void async_call(Promise<TYPE> promise) {
@@ -471,6 +483,83 @@ class AsyncProgram {
         }
     }
 
+    // Whole team: waits for the lanes' outstanding LazyLoad copies into the rings (each lane
+    // waits for its own, then the warp synchronises so every lane sees every slot).
+    __device__ __forceinline__ void settle_loads() {
+        if (*(volatile unsigned int*)&_grp_ctx.loads_pending) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            __syncwarp();
+            if (util::lane_id() == 0) _grp_ctx.loads_pending = 0;
+            __syncwarp();
+        }
+    }
+
+    // prog.async<F> with LazyLoad arguments (see async above).
+    template <typename TYPE, typename... ARGS>
+    __device__ __forceinline__ void push_lazy(ARGS... args) {
+        using Args = typename Promise<TYPE>::Args;
+        constexpr unsigned int F = disc_of<TYPE>();
+        constexpr unsigned int W = Promise<TYPE>::WORDS;
+        constexpr unsigned int SLOTS = ring_slots<F>();
+        constexpr unsigned int BASE = ring_base<F>();
+        static_assert(sizeof...(ARGS) == Promise<TYPE>::ARITY, "async: wrong number of arguments");
+        // The promise with every lazy argument left zero, and which of its words are lazy.
+        Promise<TYPE> p(hrm_rt::lazy_placeholder(args)...);
+        unsigned int w[W];
+        p.to_words(w);
+        bool lazy_word[W];
+        const unsigned int* lazy_src[W];
+#pragma unroll
+        for (unsigned int i = 0; i < W; i++) {
+            lazy_word[i] = false;
+            lazy_src[i] = nullptr;
+        }
+        hrm_rt::mark_lazy_words<Args, 0>(p.args, lazy_word, lazy_src, args...);
+        const unsigned int mask = __activemask();
+        const unsigned int rank = __popc(mask & util::lanemask_lt());
+        const unsigned int leader = __ffs(mask) - 1;
+        GroupContext& g = _grp_ctx;
+        unsigned int fits = 1u;
+        if constexpr (RING_GROUPS > 1) {
+            constexpr unsigned int G = group_of<F>();
+            if (rank == 0) {
+                unsigned int a = *(volatile unsigned int*)&g.active;
+                if (a == NO_GROUP) a = atomicCAS(&g.active, NO_GROUP, G);
+                fits = (a == NO_GROUP || a == G) ? 1u : 0u;
+            }
+            fits = __shfl_sync(mask, fits, leader);
+        }
+        unsigned int idx = SLOTS;
+        if (fits) {
+            unsigned int base = 0;
+            if (rank == 0) base = atomicAdd(&g.count[F], (unsigned int)__popc(mask));
+            base = __shfl_sync(mask, base, leader);
+            idx = base + rank;
+        }
+        const unsigned int over = __ballot_sync(mask, idx >= SLOTS);
+        if (idx < SLOTS) {
+            const unsigned int slot = (g.bottom[F] + idx) & (SLOTS - 1);
+#pragma unroll
+            for (unsigned int i = 0; i < W; i++) {
+                unsigned int* dst = &g.words[BASE + i * SLOTS + slot];
+                if (lazy_word[i]) {
+                    const unsigned int sa = (unsigned int)__cvta_generic_to_shared(dst);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(lazy_src[i]) : "memory");
+                } else {
+                    *dst = w[i];
+                }
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            g.loads_pending = 1u;
+        }
+        if (over != 0 && idx >= SLOTS) {
+            unsigned int spill_w[W];
+#pragma unroll
+            for (unsigned int i = 0; i < W; i++) spill_w[i] = lazy_word[i] ? __ldcg(lazy_src[i]) : w[i];
+            overflow_to_arena<TYPE>(spill_w, over);
+        }
+    }
+
     // Lanes in `over` could not fit in shared memory: write them straight to one arena link
     // and publish it to the function's queue. Out of line, so that every push site stays
     // small (the instruction cache is the first limit of a kernel with many async functions);
@@ -594,6 +683,7 @@ class AsyncProgram {
         constexpr unsigned int BASE = ring_base<F>();
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
+        settle_loads();
         unsigned int cnt = g.count[F];
         unsigned int n = min(cnt, nlinks * 32u);
         if (n == 0) return 0u;
@@ -701,6 +791,7 @@ class AsyncProgram {
         constexpr bool OLDEST_FIRST = hrm_rt::fn_OLDEST_FIRST<PROGRAM_SPEC, Op>::value;
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
+        settle_loads();
         const unsigned int cnt = g.count[F];
         const unsigned int bottom = g.bottom[F];
         Promise<Op> p;
@@ -787,6 +878,7 @@ class AsyncProgram {
         if (lane == 0) {
             _grp_ctx.active = NO_GROUP;
             _grp_ctx.held_n = 0;
+            _grp_ctx.loads_pending = 0;
         }
         __syncwarp();
     }

@@ -92,8 +92,10 @@ struct TaggedSemaphore {
     __host__ __device__ TaggedSemaphore(unsigned int s, unsigned int t) : sem(s), tag(t) {}
 };
 
-// Marks an argument that the original runtime could fill by an asynchronous copy
-// (promise.h:208-240). This runtime loads it eagerly.
+// Marks an argument to be filled by an asynchronous copy from global memory (promise.h:
+// 208-240 of the original, its ASYNC_LOADS form). AsyncProgram's async<F> copies such an
+// argument with cp.async into the promise's shared-memory slot; everywhere else (sync,
+// EventProgram, a promise that overflows to the arena) it converts to its value at the call.
 template <typename TYPE>
 struct LazyLoad {
     using Type = TYPE;

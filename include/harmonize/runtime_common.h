@@ -388,6 +388,49 @@ static inline unsigned int max_resident_ctas(KERNEL kernel, int threads, size_t 
     return (unsigned int)(per_sm * sms);
 }
 
+// ---------------------------------------------------------------------------------------
+// LazyLoad arguments of prog.async<F> (AsyncProgram copies them asynchronously).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct is_lazy_load : std::false_type {};
+template <typename T>
+struct is_lazy_load<LazyLoad<T>> : std::true_type {};
+
+// The value an argument contributes to the promise built at the call: a LazyLoad argument
+// contributes zero (its words are filled by the copy), any other argument itself.
+template <typename T>
+__device__ __forceinline__ T lazy_placeholder(T v) {
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T lazy_placeholder(LazyLoad<T>) {
+    static_assert(sizeof(T) % 4 == 0 && alignof(T) >= 4,
+                  "LazyLoad arguments are copied as 32-bit words: their type must be a multiple of "
+                  "4 bytes and 4-byte aligned");
+    return T{};
+}
+
+// Marks the promise words of argument I onwards that come from LazyLoad arguments, with the
+// address each word is copied from.
+template <typename ARGS, size_t I>
+__device__ __forceinline__ void mark_lazy_words(ARGS&, bool*, const unsigned int**) {}
+
+template <typename ARGS, size_t I, typename HEAD, typename... TAIL>
+__device__ __forceinline__ void mark_lazy_words(ARGS& tuple, bool* lazy, const unsigned int** src, HEAD head,
+                                                TAIL... tail) {
+    if constexpr (is_lazy_load<HEAD>::value) {
+        using T = typename HEAD::Type;
+        const size_t off = (size_t)((const char*)&TupleGet<I, ARGS>::get(tuple) - (const char*)&tuple);
+        const unsigned int* from = (const unsigned int*)&head.reference;
+#pragma unroll
+        for (unsigned int j = 0; j < sizeof(T) / 4u; j++) {
+            lazy[off / 4u + j] = true;
+            src[off / 4u + j] = from + j;
+        }
+    }
+    mark_lazy_words<ARGS, I + 1>(tuple, lazy, src, tail...);
+}
+
 }  // namespace hrm_rt
 
 #endif

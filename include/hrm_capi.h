@@ -133,6 +133,10 @@ int hrm_program_create(int spec, int program_type, size_t arena_or_io, const voi
 int hrm_program_create_variant(int spec, int program_type, int variant, size_t arena_or_io,
                                const void* device_state, size_t state_size, hrm_program** out);
 int hrm_program_destroy(hrm_program* prog);
+/* Replaces the instance's copy of the spec's device state (the next init / exec launch sees
+ * it); the original passes its DeviceState by value into every launch (program/mod.h:66), so
+ * a caller may change it between launches. */
+int hrm_program_set_state(hrm_program* prog, const void* device_state, size_t state_size);
 int hrm_program_init(hrm_program* prog, size_t groups, void* stream);
 int hrm_program_exec(hrm_program* prog, size_t groups, size_t cycles_or_chunk, void* stream);
 int hrm_program_complete(hrm_program* prog, int* out);
