@@ -64,6 +64,9 @@ struct RemappingBarrier {
     unsigned long long partial[TYPE_COUNT];      // per function: partial-link word
 
     RemappingBarrier() = default;
+    // Same as blank(sem_val) (the original's Future builds its barrier from a semaphore value,
+    // async/future.h:20-22).
+    __host__ __device__ explicit RemappingBarrier(unsigned int sem_val) : RemappingBarrier(blank(sem_val)) {}
 
     static __host__ __device__ RemappingBarrier<OP_SET, ADR_TYPE> blank(unsigned int sem_val) {
         RemappingBarrier<OP_SET, ADR_TYPE> r;
@@ -279,6 +282,53 @@ struct UnitBarrier {
     __device__ void sub_semaphore(PROGRAM program, unsigned int delta) {
         unsigned int old = atomicAdd(&semaphore.sem, (unsigned int)(0u - delta));
         if (old - delta == 0u && old != 0u) program.async_call(promise);
+    }
+};
+
+// A value tied to a barrier (async/future.h:6-33 of the original). Continuations that need
+// the value wait on the barrier with `await(prog, Promise<F>(...))`; each producer stores its
+// part and calls `fulfill(prog)`, which takes one off the barrier's semaphore, so the held
+// continuations are released once every expected producer has fulfilled (the semaphore value
+// given at construction). `set` stores the value and fulfills; `get` reads it from L2, so a
+// continuation that runs on another SM never sees a stale copy. (The original's ReturnOp,
+// future.h:37-61, which was to fill futures from returning calls, is not instantiable there;
+// producers store their results themselves.) Futures live in device memory, like barriers.
+template <typename TYPE, typename BARRIER>
+struct Future {
+    using BarrierType = BARRIER;
+    using Type = TYPE;
+    static_assert(sizeof(TYPE) % 4 == 0, "Future values are read as 32-bit words");
+
+    BarrierType barrier;
+    Type data;
+
+    Future() = default;
+    __host__ __device__ Future(unsigned int semaphore_value) : barrier(semaphore_value) {}
+
+    template <typename PROGRAM, typename OP_TYPE>
+    __device__ void await(PROGRAM program, Promise<OP_TYPE> promise) {
+        barrier.await(program, promise);
+    }
+
+    template <typename PROGRAM>
+    __device__ void fulfill(PROGRAM program) {
+        __threadfence();
+        barrier.sub_semaphore(program, 1u);
+    }
+
+    template <typename PROGRAM>
+    __device__ void set(PROGRAM program, const TYPE& value) {
+        data = value;
+        fulfill(program);
+    }
+
+    __device__ TYPE get() const {
+        TYPE v;
+        const unsigned int* src = (const unsigned int*)&data;
+        unsigned int* dst = (unsigned int*)&v;
+#pragma unroll
+        for (unsigned int i = 0; i < sizeof(TYPE) / 4u; i++) dst[i] = __ldcg(src + i);
+        return v;
     }
 };
 

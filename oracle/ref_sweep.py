@@ -35,6 +35,9 @@ def main():
     ap.add_argument("--photons", type=int, default=1_000_000)
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--max-execs", type=int, default=8000,
+                    help="give up on a shape after this many execs (the examples' shape needs about 1,400 on "
+                         "10^6 photons; a shape whose buffers overflow never completes)")
     a = ap.parse_args()
     import torch
     import oracle
@@ -55,7 +58,7 @@ def main():
         try:
             r = oracle.ref_photon_device(d_mu.data_ptr(), d_ab.data_ptr(), d_sp.data_ptr(), n, BENCH_SEED, 0, count,
                                          d_t.data_ptr(), wg=shape["wg"], nn=shape["chunk"], arena=shape["io"],
-                                         load_limit=shape["load_limit"], max_execs=400000)
+                                         load_limit=shape["load_limit"], max_execs=a.max_execs)
             ok = np.array_equal(d_t.cpu().numpy().view(np.uint64), ref)
             ms = r["ms"] if ok else float("inf")
             row = dict(shape, ms=round(r["ms"], 2), execs=r["execs"], calls_per_s=calls / (r["ms"] / 1e3),

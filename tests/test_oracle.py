@@ -149,3 +149,39 @@ def test_golden_rmat_fixture_is_the_seeded_graph():
     g = np.load(os.path.join(GOLDEN, "ref_bfs_rmat10.npz"))
     rp, col = oracle.rmat_csr(10, 16, seed=5)
     assert np.array_equal(g["rowptr"], rp) and np.array_equal(g["col"], col)
+
+
+def _sha256(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_collatz_full_range_matches_reference_runtime_digest():
+    """n = 1..2^20, the Collatz benchmark range: the reference AsyncProgram's stopping times
+    (digest in tests/golden/ref_collatz_1_2p20.json) equal the restated checker's."""
+    import json
+    g = json.load(open(os.path.join(GOLDEN, "ref_collatz_1_2p20.json")))
+    steps = oracle.collatz_range(g["start"], g["count"])
+    assert int(steps.astype(np.uint64).sum()) == g["sum"] and int(steps.max()) == g["max"]
+    assert _sha256(steps.astype(np.uint32)) == g["sha256"]
+
+
+def test_photon_bench_medium_matches_reference_runtime_digest():
+    """10^4 photons of the bench walk (128^3 medium, seed 2024; walk seed 0x5EED0123456789)
+    through the reference EventProgram: the restated walk gives the same tallies, byte for byte."""
+    import json
+    g = json.load(open(os.path.join(GOLDEN, "ref_photon_n128_1e4.json")))
+    mu, ab, sp = oracle.photon_medium(g["n"], g["medium_seed"])
+    t, _ = oracle.photon_walk(mu, ab, sp, g["n"], g["seed"], g["first"], g["count"])
+    v, s = g["n"] ** 3, oracle.PHOTON_SPREAD
+    assert int(np.count_nonzero(t)) == g["nonzero"]
+    assert int(t[:v].astype(object).sum()) == g["voxels"]
+    assert int(t[v + s:v + 2 * s].astype(object).sum()) == g["killed"]
+    assert int(t[v + 2 * s:].astype(object).sum()) == g["gained"]
+    assert _sha256(t) == g["sha256"]
+
+
+def test_bfs_rmat16_matches_reference_runtime_output():
+    g = np.load(os.path.join(GOLDEN, "ref_bfs_rmat16_levels.npz"))
+    rp, col = oracle.rmat_csr(int(g["scale"]), int(g["edge_factor"]), seed=int(g["seed"]))
+    assert np.array_equal(oracle.bfs(rp, col, int(g["root"])), g["levels"])
