@@ -54,7 +54,9 @@ class RunConfig(ctypes.Structure):
 
 
 # Compiled tuning variants: (shared-memory ring links per function, teams per CTA).
-VARIANTS = {0: (2, 4), 1: (4, 4), 2: (4, 2), 3: (8, 2), 4: (2, 8)}
+# (ring links per function, teams per CTA); the lean variants give the first function 4 links
+# and the others 2, and are compiled for at least 10 / 11 resident CTAs per SM.
+VARIANTS = {0: (2, 4), 1: (4, 4), 2: (4, 2), 3: (8, 2), 4: (2, 8), 5: (4, 2), 6: (4, 2)}
 
 
 class RunResult(ctypes.Structure):

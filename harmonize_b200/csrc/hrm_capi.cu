@@ -99,6 +99,19 @@ STATE state_from(const void* p, size_t n) {
     return s;
 }
 
+// Tuning adapter of the "lean" variants: the spec's first async function keeps rings of BIG
+// links, every other function gets SMALL links, and the kernel is compiled for at least
+// MIN_CTAS resident CTAs per SM (__launch_bounds__). Smaller rings for the functions that a
+// batch of the first one feeds leave shared memory for more teams per SM.
+template <class BASE, size_t BIG, size_t SMALL, size_t MIN_CTAS>
+struct LeanRings : BASE {
+    static const size_t MIN_CTAS_PER_SM = MIN_CTAS;
+    template <typename Op>
+    struct RING_LINKS_OF {
+        static const size_t value = std::is_same<Op, typename OpAt<0, typename BASE::OpSet>::type>::value ? BIG : SMALL;
+    };
+};
+
 // Instantiates spec SPEC<RING, TEAMS> for the chosen program type and tuning variant.
 template <template <size_t, size_t> class SPEC, typename STATE>
 ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
@@ -109,6 +122,8 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_R4_T2: return new ProgramImpl<AsyncProgram<SPEC<4, 2>>>(arena, s);
             case HRM_VARIANT_R8_T2: return new ProgramImpl<AsyncProgram<SPEC<8, 2>>>(arena, s);
             case HRM_VARIANT_R2_T8: return new ProgramImpl<AsyncProgram<SPEC<2, 8>>>(arena, s);
+            case HRM_VARIANT_LEAN_T2_M10: return new ProgramImpl<AsyncProgram<LeanRings<SPEC<4, 2>, 4, 2, 10>>>(arena, s);
+            case HRM_VARIANT_LEAN_T2_M11: return new ProgramImpl<AsyncProgram<LeanRings<SPEC<4, 2>, 4, 2, 11>>>(arena, s);
             default: break;
         }
     } else if (type == HRM_EVENT) {
@@ -116,7 +131,9 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_R2_T4:
             case HRM_VARIANT_R4_T4: return new ProgramImpl<EventProgram<SPEC<2, 4>>>(arena, s);
             case HRM_VARIANT_R4_T2:
-            case HRM_VARIANT_R8_T2: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
+            case HRM_VARIANT_R8_T2:
+            case HRM_VARIANT_LEAN_T2_M10:
+            case HRM_VARIANT_LEAN_T2_M11: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
             case HRM_VARIANT_R2_T8: return new ProgramImpl<EventProgram<SPEC<2, 8>>>(arena, s);
             default: break;
         }

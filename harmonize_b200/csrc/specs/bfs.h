@@ -43,8 +43,9 @@ struct BfsExpand {
     HRM_DEV static void eval(PROGRAM prog, unsigned int level, unsigned int begin, unsigned int end) {
 #if defined(__CUDA_ARCH__)
         // The runtimes evaluate a batch as `if (lane < k) eval(...)`: the active lanes are
-        // 0 .. k-1, which the flattened walk below relies on; any other lane set walks lane
-        // by lane.
+        // 0 .. k-1, which the flattened walk below relies on. The lanes must also share one
+        // search (a batch of the job-multiplexing runtime can hold Expand calls of several
+        // jobs, each with its own graph, levels and queues): any other batch walks lane by lane.
         const unsigned int mask = __activemask();
         const bool split = end - begin > BFS_CHUNK;
         if (split) {
@@ -53,7 +54,11 @@ struct BfsExpand {
             prog.template async<BfsExpand>(level, mid, end);
         }
         __syncwarp(mask);
-        if ((mask & (mask + 1u)) == 0u) {
+        // (One search = one graph and one levels array: every job writes its own levels.)
+        int same_col = 0, same_levels = 0;
+        __match_all_sync(mask, (unsigned long long)(uintptr_t)prog.device.col, &same_col);
+        __match_all_sync(mask, (unsigned long long)(uintptr_t)prog.device.levels, &same_levels);
+        if ((mask & (mask + 1u)) == 0u && same_col && same_levels) {
             expand_flat(prog, mask, level, begin, split ? 0u : end - begin);
             return;
         }

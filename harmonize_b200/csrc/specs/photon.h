@@ -124,8 +124,21 @@ HRM_HD HRM_FI unsigned long long child_id(unsigned long long id, unsigned int st
     return hrm::mix64(id ^ (((unsigned long long)step << 1) | c) * 0x9E3779B97F4A7C15ull);
 }
 
-// Voxel index -> (ix, iy, iz) with two divisions: v / (n*n) == (v / n) / n for unsigned v.
+// Voxel index -> (ix, iy, iz): shifts and masks when n is a power of two (the same value for
+// every lane of a batch, so the test does not diverge), else two divisions
+// (v / (n*n) == (v / n) / n for unsigned v).
 HRM_HD HRM_FI void voxel_coords(unsigned int v, unsigned int n, unsigned int& ix, unsigned int& iy, unsigned int& iz) {
+    if ((n & (n - 1u)) == 0u) {
+#if defined(__CUDA_ARCH__)
+        const unsigned int s = (unsigned int)(__ffs((int)n) - 1);
+#else
+        const unsigned int s = (unsigned int)__builtin_ctz(n);
+#endif
+        ix = v & (n - 1u);
+        iy = (v >> s) & (n - 1u);
+        iz = v >> (2u * s);
+        return;
+    }
     const unsigned int q = v / n;
     ix = v - q * n;
     iz = q / n;

@@ -100,7 +100,11 @@ typedef struct hrm_run_config {
 #define HRM_VARIANT_R4_T2 2
 #define HRM_VARIANT_R8_T2 3
 #define HRM_VARIANT_R2_T8 4
-#define HRM_VARIANT_COUNT 5
+/* Lean rings: the spec's first async function 4 links, the others 2, 2 teams per CTA, compiled
+ * for at least 10 (M10) or 11 (M11) resident CTAs per SM (more teams per SM, fewer registers). */
+#define HRM_VARIANT_LEAN_T2_M10 5
+#define HRM_VARIANT_LEAN_T2_M11 6
+#define HRM_VARIANT_COUNT 7
 
 /* What a whole run reports back. */
 typedef struct hrm_run_result {

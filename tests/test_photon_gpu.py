@@ -40,7 +40,7 @@ def test_photon_zero_photons(hrm, medium16):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", range(5))
+@pytest.mark.parametrize("variant", range(7))
 def test_every_compiled_variant_matches_oracle(hrm, medium16, variant):
     """Every compiled tuning variant (ring links per function, teams per CTA) gives
     the same tallies and call count for all three specs."""
