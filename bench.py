@@ -207,7 +207,8 @@ def flush_l2(buf):
 #   photon Collide : 2 x 44 B promise + 4 B absorb                          =  92 B
 #   photon Tally   : 2 x 16 B promise + 16 B uint64 read-modify-write       =  48 B
 #   BFS Relax      : 2 x 8 B promise + 8 B level read-modify-write          =  24 B
-#   BFS Expand     : 2 x 12 B promise + 8 B rowptr + 4 B per edge read (counted on Relax side: 4 B)
+#   BFS Expand     : 2 x 16 B promise + 8 B rowptr + 4 B level of the expanded vertex      =  44 B
+#                    (the 4 B column read per edge is counted on the Relax side)
 #   Collatz Even/Odd: 2 x 16 B promise (+ 4 B output once per start, ignored) = 32 B
 # ---------------------------------------------------------------------------------------
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one exec launch on a
@@ -217,7 +218,7 @@ TRAFFIC_PROFILE = {("photon", "async"): (2631936 + 375808, 161486336)}
 
 BYTES_PER_CALL = {
     "photon": [93, 92, 48],
-    "bfs": [24 + 4, 24 + 8],
+    "bfs": [24 + 4, 32 + 8 + 4],
     "collatz": [32, 32],
 }
 

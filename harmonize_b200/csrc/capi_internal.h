@@ -15,6 +15,10 @@ namespace hrm_capi {
 // Records `msg` as the calling thread's last error (read by hrm_last_error) and returns code.
 int set_error(int code, const std::string& msg);
 
+// Teams (32-lane work groups) of the single-spec photon-walk AsyncProgram of tuning variant
+// `variant` that can be resident on one SM of the current device at once.
+unsigned int photon_teams_per_sm(int variant);
+
 // Two timing events, destroyed on every path out of the scope that made them (a failed
 // launch or a device error flag throws between record and read).
 struct EventPair {

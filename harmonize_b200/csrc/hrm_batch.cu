@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstddef>
 #include <deque>
 #include <map>
@@ -388,6 +389,9 @@ struct ServerBase {
     virtual unsigned int poll(uint64_t* done_ns, unsigned int max) = 0;    // returns completed count
     virtual void close(unsigned int timeout_ms) = 0;
     virtual size_t arena_bytes() const = 0;
+    // Free arena bytes as the device sees them now: links never handed out plus links on the
+    // free-link ring, read from the running instance's control block and ring head.
+    virtual size_t observed_free_bytes() = 0;
     virtual std::string describe_unfinished() = 0;
     virtual volatile unsigned long long* done_flags() = 0;
     virtual std::string error() = 0;
@@ -412,16 +416,29 @@ struct Server : ServerBase {
     std::string err;
     std::mutex submit_lock;
     size_t arena_links;
-    // Solo lane: photon jobs of at least solo_photons photons fill the GPU on their own and run
-    // at about half speed inside the multiplexing kernel, so the session serves them alone
-    // through the single-spec runtime: submit queues them and halts the running exec (teams
-    // spill their work and leave within a few scheduling rounds); the runner serves the queue
-    // in submission order between execs, then resumes the persistent kernel, whose state
-    // waited in the arena. Their job records are placeholders with an empty source, which the
-    // kernel closes and never works on.
+    // Solo lane, partitioned residency: photon jobs of at least solo_photons photons fill the
+    // GPU on their own and run at about half speed inside the multiplexing kernel, so the
+    // session serves them through the single-spec runtime, BESIDE the resident kernel: while
+    // a solo job is queued or running, the resident kernel is launched with half of its teams
+    // per SM (half_groups) and the solo job's kernel with half of its own (solo_groups), so
+    // both are resident at once and the small jobs keep flowing. With no solo work the
+    // resident kernel runs with all its teams. submit queues a solo job and, if the resident
+    // exec on the GPU holds every team, halts it (teams spill their work and leave within a
+    // few scheduling rounds) so that the runner relaunches it with half; the solo runner
+    // halts the half-share exec once the queue drains, so that it comes back with all teams.
+    // A solo job's record is a placeholder with an empty source, which the kernel closes and
+    // never works on; its completion is stamped by the solo runner.
     unsigned int solo_photons;
-    std::mutex solo_lock;
+    std::mutex solo_lock;                                     // guards the fields below
+    std::condition_variable solo_cv;
     std::deque<std::pair<unsigned int, hrm_job>> solo_queue;  // (job index, job)
+    bool solo_running = false;                                // a solo job is on the GPU
+    bool exec_half = false;                                   // the exec on the GPU holds half the teams
+    bool exec_on_gpu = false;                                 // a resident exec is launched
+    bool solo_exit = false;                                   // the solo runner should stop
+    size_t half_groups = 0, solo_groups = 0;
+    cudaStream_t solo_s = nullptr;
+    std::thread solo_runner;
     unsigned long long* done_dev = nullptr;                    // device alias of done_host
 
     Server(unsigned int cap, const hrm_run_config& cfg)
@@ -440,6 +457,7 @@ struct Server : ServerBase {
             throw;
         }
         runner = std::thread([this] { loop(); });
+        if (solo_photons) solo_runner = std::thread([this] { solo_loop(); });
     }
 
     void set_up(unsigned int cap, const hrm_run_config& cfg) {
@@ -471,11 +489,41 @@ struct Server : ServerBase {
         mix_prepare_range_kernel<<<1, 32, 0, submit_s>>>(jobs.data(), 0u, 0u);
         ck(cudaGetLastError(), "kernel load");
         ck(cudaStreamSynchronize(submit_s), "kernel load");
+        if (solo_photons) {
+            // Half of each kernel's resident teams per SM: two halves fit one SM together.
+            ck(cudaStreamCreateWithFlags(&solo_s, cudaStreamNonBlocking), "stream");
+            int dev = 0, sms = 1;
+            ck(cudaGetDevice(&dev), "cudaGetDevice");
+            ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+            const unsigned int mix_ctas_per_sm = P::resident_ctas() / (unsigned int)sms;
+            const unsigned int solo_teams_per_sm = hrm_capi::photon_teams_per_sm(HRM_VARIANT_R4_T2);
+            half_groups = (size_t)std::max(1u, mix_ctas_per_sm / 2u) * (size_t)sms * P::TEAMS_PER_CTA;
+            solo_groups = (size_t)std::max(2u, (solo_teams_per_sm / 2u) & ~1u) * (size_t)sms;
+            // The solo job's kernel must start before the half-share exec may be counted on:
+            // load it now (lazy loading would hold it back until a running kernel ends).
+            hrm_run_config c;
+            memset(&c, 0, sizeof(c));
+            c.program_type = HRM_ASYNC;
+            c.variant = HRM_VARIANT_R4_T2;
+            c.stream = solo_s;
+            c.groups = solo_groups;
+            util::host::DevBuf<float> m((size_t)8);
+            util::host::DevBuf<unsigned char> sp((size_t)8);
+            util::host::DevBuf<unsigned long long> t((size_t)(8 + 3 * hrm_specs::PHOTON_SPREAD));
+            ck(cudaMemset(m.data(), 0, 8 * sizeof(float)), "warm-up medium");
+            ck(cudaMemset(sp.data(), 0, 8), "warm-up medium");
+            hrm_run_result r;
+            if (hrm_photon_run_device(m.data(), m.data(), sp.data(), 2, 1, 0, 0, (uint64_t*)t.data(), &c, &r) != HRM_OK)
+                throw std::runtime_error(std::string("solo lane warm-up: ") + hrm_last_error());
+            ck(cudaFuncGetAttributes(&fa, stamp_done_kernel), "kernel load");
+        }
     }
 
     void release_host_resources() {
         if (exec_s) cudaStreamDestroy(exec_s);
         if (submit_s) cudaStreamDestroy(submit_s);
+        if (solo_s) cudaStreamDestroy(solo_s);
+        solo_s = nullptr;
         if (done_host) cudaFreeHost(done_host);
         if (staging) cudaFreeHost(staging);
         if (pinned_ctr) cudaFreeHost(pinned_ctr);
@@ -498,57 +546,107 @@ struct Server : ServerBase {
             cudaStreamSynchronize(submit_s);
             runner.join();
         }
+        stop_solo_runner();
         release_host_resources();
     }
 
-    // Relaunches the persistent kernel until the session is closed and every job is done.
-    bool pop_solo(std::pair<unsigned int, hrm_job>& out) {
-        std::lock_guard<std::mutex> g(solo_lock);
-        if (solo_queue.empty()) return false;
-        out = solo_queue.front();
-        solo_queue.pop_front();
-        return true;
+    void stop_solo_runner() {
+        {
+            std::lock_guard<std::mutex> g(solo_lock);
+            solo_exit = true;
+        }
+        solo_cv.notify_all();
+        if (solo_runner.joinable()) solo_runner.join();
     }
 
-    // One queued solo job, on the exec stream while the persistent kernel is not running.
+    void halt_resident() {
+        halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
+        ck(cudaGetLastError(), "halt");
+        ck(cudaStreamSynchronize(submit_s), "halt");
+    }
+
+    // One solo job on the solo stream, beside the half-share resident exec.
     void run_solo(unsigned int j, const hrm_job& jb) {
         hrm_run_config c;
         memset(&c, 0, sizeof(c));
         c.program_type = HRM_ASYNC;
         c.variant = HRM_VARIANT_R4_T2;  // the photon walk's tuned variant on this GPU
-        c.stream = exec_s;
+        c.stream = solo_s;
+        c.groups = solo_groups;
         hrm_run_result r;
         if (hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
                                   jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
             throw std::runtime_error(std::string("solo photon job: ") + hrm_last_error());
-        stamp_done_kernel<<<1, 32, 0, exec_s>>>(done_dev, j);
+        stamp_done_kernel<<<1, 32, 0, solo_s>>>(done_dev, j);
         ck(cudaGetLastError(), "solo stamp");
-        ck(cudaStreamSynchronize(exec_s), "solo stamp");
+        ck(cudaStreamSynchronize(solo_s), "solo stamp");
     }
 
+    // The solo runner: serves the solo queue in submission order, one job at a time, only
+    // while the resident exec holds half of its teams (or no resident exec is running).
+    void solo_loop() {
+        try {
+            while (true) {
+                std::pair<unsigned int, hrm_job> sj;
+                {
+                    std::unique_lock<std::mutex> g(solo_lock);
+                    solo_cv.wait_for(g, std::chrono::milliseconds(2), [this] {
+                        return solo_exit || (!solo_queue.empty() && (exec_half || !exec_on_gpu));
+                    });
+                    if (solo_exit) break;
+                    if (solo_queue.empty() || !(exec_half || !exec_on_gpu)) continue;
+                    sj = solo_queue.front();
+                    solo_queue.pop_front();
+                    solo_running = true;
+                }
+                run_solo(sj.first, sj.second);
+                bool drained;
+                {
+                    std::lock_guard<std::mutex> g(solo_lock);
+                    solo_running = false;
+                    drained = solo_queue.empty() && exec_on_gpu && exec_half;
+                }
+                // Nothing left for the solo lane: give the resident exec all its teams back.
+                if (drained) halt_resident();
+            }
+        } catch (std::exception& e) {
+            std::lock_guard<std::mutex> g(err_lock);
+            err = e.what();
+        }
+    }
+
+    // Relaunches the persistent kernel until the session is closed and every job is done.
     void loop() {
         try {
             while (true) {
                 if (stop) break;
-                // Clear a served halt request, then look at the solo queue: submit queues a
-                // job before it requests the halt, so a job queued after this look comes with
-                // a halt that lands after this clear and stops the exec launched below.
+                // Clear a served halt request, then look at the solo lane: submit queues a job
+                // before it requests the halt, so a job queued after this look comes with a
+                // halt that lands after this clear and stops the exec launched below.
                 ck(cudaMemsetAsync(&inst.control.data()->flags, 0, sizeof(unsigned int), exec_s), "clear flags");
                 ck(cudaStreamSynchronize(exec_s), "clear flags");
-                std::pair<unsigned int, hrm_job> sj;
-                if (pop_solo(sj)) {
-                    run_solo(sj.first, sj.second);
-                    continue;
+                bool half;
+                {
+                    std::lock_guard<std::mutex> g(solo_lock);
+                    half = solo_photons && (!solo_queue.empty() || solo_running);
+                    exec_half = half;
+                    exec_on_gpu = true;
                 }
-                P::launch_exec(inst, groups, cycles, exec_s);
-                ck(cudaStreamSynchronize(exec_s), "serving exec");
+                solo_cv.notify_all();
+                P::launch_exec(inst, half ? half_groups : groups, cycles, exec_s);
+                cudaError_t le = cudaStreamSynchronize(exec_s);
+                {
+                    std::lock_guard<std::mutex> g(solo_lock);
+                    exec_on_gpu = false;
+                }
+                ck(le, "serving exec");
                 unsigned int f = inst.flags();
                 if (f & hrm_rt::ERROR_MASK) hrm_rt::throw_flags(f);
                 if (stop) break;
                 bool solo_left;
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
-                    solo_left = !solo_queue.empty();
+                    solo_left = !solo_queue.empty() || solo_running;
                 }
                 if (!host_open && (f & hrm_rt::COMPLETION_FLAG) && !solo_left) break;
             }
@@ -590,14 +688,16 @@ struct Server : ServerBase {
         ck(cudaStreamSynchronize(submit_s), "admit");
         submitted = first + n;
         if (!solo.empty()) {
+            bool full_on_gpu;
             {
                 std::lock_guard<std::mutex> g(solo_lock);
                 for (auto& s : solo) solo_queue.push_back(s);
+                full_on_gpu = exec_on_gpu && !exec_half;
             }
-            // Queued first, then the halt: see loop().
-            halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
-            ck(cudaGetLastError(), "solo halt");
-            ck(cudaStreamSynchronize(submit_s), "solo halt");
+            solo_cv.notify_all();
+            // Queued first, then the halt (see loop()): the exec holding every team leaves and
+            // comes back with half of them.
+            if (full_on_gpu) halt_resident();
         }
         return first;
     }
@@ -629,6 +729,7 @@ struct Server : ServerBase {
             if (!e.empty()) throw std::runtime_error(e);
         }
         if (runner.joinable()) runner.join();
+        stop_solo_runner();
         std::string e = error();
         if (!e.empty()) throw std::runtime_error(e);
     }
@@ -658,6 +759,18 @@ struct Server : ServerBase {
     }
 
     size_t arena_bytes() const override { return arena_links * P::LINK_WORDS * 128u; }
+    size_t observed_free_bytes() override {
+        // Two 4-byte reads on the submit stream; the copy engine reads them through L2 while
+        // the persistent kernel runs.
+        ck(cudaMemcpyAsync(pinned_ctr + 4, &inst.control.data()->bump, 4, cudaMemcpyDeviceToHost, submit_s), "bump");
+        ck(cudaMemcpyAsync(pinned_ctr + 5, &inst.heads.data()[P::FN].avail, 4, cudaMemcpyDeviceToHost, submit_s),
+           "free links");
+        ck(cudaStreamSynchronize(submit_s), "free arena read");
+        const size_t bump = std::min<size_t>(pinned_ctr[4], arena_links);
+        const int on_ring = (int)pinned_ctr[5];
+        const size_t free_links = (arena_links - bump) + (size_t)(on_ring > 0 ? on_ring : 0);
+        return free_links * P::LINK_WORDS * 128u;
+    }
     volatile unsigned long long* done_flags() override { return done_host; }
     std::string error() override {
         std::lock_guard<std::mutex> g(err_lock);
@@ -745,8 +858,8 @@ int hrm_server_destroy(hrm_server* srv) {
 }
 
 // Replays an arrival schedule: arrival_ns[j] (non-decreasing, from the start of the call).
-// mode 0: the resident runtime (a server session, jobs admitted FIFO while their estimated
-// arena bytes fit half of the arena); mode 1: one plain launch per job at its arrival, on
+// mode 0: the resident runtime (a server session, jobs admitted FIFO while the device reports
+// at least a quarter of the arena free and their estimated arena bytes fit half of it); mode 1: one plain launch per job at its arrival, on
 // nstreams streams. latency_ns[j] = host-observed completion - arrival.
 int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int mode, uint32_t nstreams,
                      const hrm_run_config* cfg_in, uint64_t* latency_ns, float* makespan_ms) {
@@ -766,6 +879,11 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
         if (mode == 0) {
             std::unique_ptr<ServerBase> srv(make_server(njobs ? njobs : 1, cfg));
             const size_t budget = srv->arena_bytes() / 2;
+            // Admission by free arena bytes: a job is admitted while the arena the device
+            // reports free stays above a quarter of it, and while the estimated footprints of
+            // the jobs in flight fit half of it (the estimate covers jobs admitted since the
+            // last read, whose promises the device has not counted yet).
+            const size_t free_floor = srv->arena_bytes() / 4;
             volatile unsigned long long* done = srv->done_flags();
             std::vector<uint32_t> inflight;
             size_t used = 0;
@@ -779,9 +897,11 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
                                              " of " + std::to_string(njobs) + " done" + srv->describe_unfinished());
                 }
                 batch.clear();
+                const bool arrivals = admitted < njobs && arrival_ns[admitted] <= now;
+                const size_t free_now = arrivals ? srv->observed_free_bytes() : 0;
                 while (admitted < njobs && arrival_ns[admitted] <= now) {
                     size_t fp = job_footprint(jobs[admitted]);
-                    if (used + fp > budget && !inflight.empty()) break;
+                    if ((used + fp > budget || free_now < free_floor) && !inflight.empty()) break;
                     used += fp;
                     batch.push_back(jobs[admitted]);
                     inflight.push_back(admitted);

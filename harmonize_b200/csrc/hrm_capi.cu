@@ -446,6 +446,23 @@ struct hrm_program {
 
 int hrm_capi::set_error(int code, const std::string& msg) { return fail(code, msg); }
 
+unsigned int hrm_capi::photon_teams_per_sm(int variant) {
+    int dev = 0, sms = 1;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    unsigned int ctas = 0, teams = 0;
+    switch (variant) {
+        case HRM_VARIANT_R4_T2: {
+            using P = AsyncProgram<hrm_specs::PhotonSpec<4, 2>>;
+            ctas = P::resident_ctas();
+            teams = P::TEAMS_PER_CTA;
+            break;
+        }
+        default: throw std::invalid_argument("photon_teams_per_sm: variant not supported");
+    }
+    return (ctas / (unsigned int)(sms > 0 ? sms : 1)) * teams;
+}
+
 #define HRM_GUARD(...)                                           \
     try {                                                        \
         __VA_ARGS__                                              \

@@ -5,10 +5,13 @@
 //  * Relax(v, l): atomicMin(levels[v], l); if that lowered the level, expand v's edges at
 //    level l+1. A vertex can be relaxed more than once (label correcting); the final
 //    levels equal the serial BFS distances whatever the order of evaluation.
-//  * Expand(l, begin, end): ranges longer than BFS_CHUNK edges are halved into two Expand
-//    calls (so high-degree vertices spread over many lanes); shorter ranges call Relax once
-//    per edge whose target currently holds a level above l (one async call per edge
-//    relaxation; the read is a filter only, atomicMin decides).
+//  * Expand(l, begin, end, v): the edges [begin, end) of vertex v at level l. If v's level
+//    has dropped below l - 1 since (a smaller level reached it and a newer Expand covers the
+//    same edges with a smaller level), the call is stale and does nothing. Otherwise ranges
+//    longer than BFS_CHUNK edges are halved into two Expand calls (so high-degree vertices
+//    spread over many lanes); shorter ranges call Relax once per edge whose target currently
+//    holds a level above l (one async call per edge relaxation; the read is a filter only,
+//    atomicMin decides).
 //    On the GPU the lanes of a batch that evaluate Expand together walk their short ranges
 //    as one flattened edge list: lane L takes edge L, L+k, ... of the concatenation (k =
 //    lanes in the batch), so the col reads of a warp are consecutive addresses and the
@@ -38,9 +41,12 @@ struct BfsRelax;
 struct BfsExpand;
 
 struct BfsExpand {
-    using Type = void (*)(unsigned int, unsigned int, unsigned int);
+    using Type = void (*)(unsigned int, unsigned int, unsigned int, unsigned int);
     template <typename PROGRAM>
-    HRM_DEV static void eval(PROGRAM prog, unsigned int level, unsigned int begin, unsigned int end) {
+    HRM_DEV static void eval(PROGRAM prog, unsigned int level, unsigned int begin, unsigned int end, unsigned int v) {
+        // Stale: v holds a level below level - 1, so its newer Expand relaxes these edges with
+        // a smaller level (this one would only make corrections that the newer one undoes).
+        if (hrm::load_relaxed_u32(&prog.device.levels[v]) + 1u < level) end = begin;
 #if defined(__CUDA_ARCH__)
         // The runtimes evaluate a batch as `if (lane < k) eval(...)`: the active lanes are
         // 0 .. k-1, which the flattened walk below relies on. The lanes must also share one
@@ -50,8 +56,8 @@ struct BfsExpand {
         const bool split = end - begin > BFS_CHUNK;
         if (split) {
             unsigned int mid = begin + (end - begin) / 2u;
-            prog.template async<BfsExpand>(level, begin, mid);
-            prog.template async<BfsExpand>(level, mid, end);
+            prog.template async<BfsExpand>(level, begin, mid, v);
+            prog.template async<BfsExpand>(level, mid, end, v);
         }
         __syncwarp(mask);
         // (One search = one graph and one levels array: every job writes its own levels.)
@@ -66,8 +72,8 @@ struct BfsExpand {
 #else
         if (end - begin > BFS_CHUNK) {
             unsigned int mid = begin + (end - begin) / 2u;
-            prog.template async<BfsExpand>(level, begin, mid);
-            prog.template async<BfsExpand>(level, mid, end);
+            prog.template async<BfsExpand>(level, begin, mid, v);
+            prog.template async<BfsExpand>(level, mid, end, v);
             return;
         }
 #endif
@@ -130,7 +136,7 @@ struct BfsRelax {
         unsigned int old = hrm::atomic_min_u32(&prog.device.levels[v], level);
         if (level < old) {
             unsigned int b = prog.device.rowptr[v], e = prog.device.rowptr[v + 1u];
-            if (e > b) prog.template async<BfsExpand>(level + 1u, b, e);
+            if (e > b) prog.template async<BfsExpand>(level + 1u, b, e, v);
         }
     }
 };

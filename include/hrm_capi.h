@@ -286,8 +286,8 @@ int hrm_server_poll(hrm_server* srv, uint64_t* done_ns, uint32_t max, uint32_t* 
 int hrm_server_close(hrm_server* srv, uint32_t timeout_ms);
 int hrm_server_destroy(hrm_server* srv);
 /* Replays an arrival schedule (arrival_ns[j], non-decreasing, from the start of the call):
- * mode 0 = the resident runtime (jobs admitted FIFO while their estimated arena bytes fit in
- * half of the arena), mode 1 = one plain launch per job at its arrival on nstreams streams.
+ * mode 0 = the resident runtime (jobs admitted FIFO while the free arena the device reports
+ * stays above a quarter of the arena and their estimated arena bytes fit in half of it), mode 1 = one plain launch per job at its arrival on nstreams streams.
  * latency_ns[j] = host-observed completion minus arrival; *makespan_ms = time to the last. */
 int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arrival_ns, int mode, uint32_t nstreams,
                      const hrm_run_config* cfg, uint64_t* latency_ns, float* makespan_ms);

@@ -206,7 +206,7 @@ REF_ASYNC_CLOSED_BFS = ("reference AsyncProgram not run on BFS: its Expand evals
 
 # Launch shape of the reference EventProgram on the photon walk: the best of the sweep in
 # profiles/reference_eventprogram_photon_sweep.txt (oracle/ref_sweep.py).
-REF_PHOTON_SHAPE = {"wg": REF_WG, "chunk": 1, "io": 1 << 24, "load_limit": 1.0 / 64}
+REF_PHOTON_SHAPE = {"wg": 148 * 32, "chunk": 4, "io": 1 << 24, "load_limit": 1.0 / 64}
 
 
 def ref_photon_device(d_mu, d_ab, d_sp, n, seed, first, count, d_tally, program="event", wg=None, nn=None,
