@@ -83,8 +83,6 @@ class AsyncProgram {
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
     static const unsigned int COALESCE_PATIENCE =
         (unsigned int)hrm_rt::spec_COALESCE_PATIENCE<PROGRAM_SPEC>::value;
-    static const unsigned int BURST = (unsigned int)hrm_rt::spec_BURST<PROGRAM_SPEC>::value;
-    static_assert(BURST >= 1, "BURST must be at least 1");
 
     static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
     static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
@@ -1059,23 +1057,6 @@ class AsyncProgram {
             n_batches += 1;
             n_full += (k == 32u);
             if (lane == bf) fn_evals += k;
-            // Burst: more full batches of the same function, without a scheduling step between
-            // them, while it holds one and every other ring keeps a batch's worth of room.
-            if (k == 32u && !forced) {
-                for (unsigned int rep = 1; rep < BURST; rep++) {
-                    const unsigned int cn = (lane < FN) ? g.count[lane] : 0u;
-                    if (__shfl_sync(0xFFFFFFFFu, cn, bf) < 32u) break;
-                    if (__any_sync(0xFFFFFFFFu, lane < FN && lane != bf && cn > my_ring - 32u)) break;
-                    run_fn<0>(bf, 32u);
-                    hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
-                    publish_held();
-                    clamp_counts();
-                    n_evals += 32u;
-                    n_batches += 1;
-                    n_full += 1;
-                    if (lane == bf) fn_evals += 32u;
-                }
-            }
         }
 
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
