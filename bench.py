@@ -204,8 +204,9 @@ def flush_l2(buf):
 # Algorithmic bytes per call (roofline accounting). A queued promise is written once and
 # read once; each function then touches its compulsory application bytes.
 #   photon Move    : 2 x 44 B promise + 4 B mu_s + 1 B split flag          =  93 B
-#   photon Collide : 2 x 44 B promise + 4 B absorb                          =  92 B
-#   photon Tally   : 2 x 16 B promise + 16 B uint64 read-modify-write       =  48 B
+#   photon Collide : 2 x 32 B promise (no direction) + 4 B absorb          =  68 B
+#   photon Tally   : 2 x 8 B promise (slot and amount in one word)
+#                    + 16 B uint64 read-modify-write                       =  32 B
 #   BFS Relax      : 2 x 8 B promise + 8 B level read-modify-write          =  24 B
 #   BFS Expand     : 2 x 16 B promise + 8 B rowptr + 4 B level of the expanded vertex      =  44 B
 #                    (the 4 B column read per edge is counted on the Relax side)
@@ -217,7 +218,7 @@ def flush_l2(buf):
 TRAFFIC_PROFILE = {("photon", "async"): (2631936 + 375808, 161486336)}
 
 BYTES_PER_CALL = {
-    "photon": [93, 92, 48],
+    "photon": [93, 68, 32],
     "bfs": [24 + 4, 32 + 8 + 4],
     "collatz": [32, 32],
 }
@@ -275,7 +276,28 @@ def run_photon(args, hrm, rank, world, pg, torch):
                          f"same spec source, {int(calls.sum())} calls in {dt:.1f} s"}
         return np.array_equal(got, ref), cpu
 
+    def plain_arm(flush):
+        """The same photons through the plain kernel (one thread per source photon, walking its
+        split descendants on a per-thread stack; no runtime), best of three with L2 flushed,
+        and whether its tallies equal the timed run's. Outside the timed region."""
+        from harmonize_b200 import jobs
+        d_plain = torch.zeros(slots, dtype=torch.int64, device="cuda")
+        arr = (jobs.Job * 1)()
+        arr[0] = jobs.Job(jobs.JOB_PHOTON, first, count, n, seed, d_mu.data_ptr(), d_ab.data_ptr(), d_sp.data_ptr(),
+                          d_plain.data_ptr())
+        JL = jobs._bind()
+        best = None
+        for _ in range(3):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            done = np.zeros(1, dtype=np.uint64)
+            total = ctypes.c_float()
+            hrm.check(JL.hrm_plain_run(ctypes.byref(arr), 1, 1, done.ctypes.data, ctypes.byref(total)))
+            best = total.value if best is None else min(best, total.value)
+        return best, bool(torch.equal(d_plain, d_tally))
+
     return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
+                plain_arm=plain_arm,
                 h2d=int(mu.nbytes + ab.nbytes + sp.nbytes), d2h=int(slots * 8), dtype="f32",
                 bytes_per_call=BYTES_PER_CALL["photon"], launches_per_step=3 if args.program == "async" else 2)
 
@@ -545,6 +567,16 @@ def main():
     e2e_calls = sum_over_ranks(pg, st["evals"] * e2e_steps)
     e2e_value = e2e_calls / (e2e_total / 1e3)
 
+    # Rank 0: the plain one-thread-per-photon kernel on the same photons (not a bench arm: the
+    # runtime's non-runtime baseline, outside the timed region).
+    plain = None
+    if rank == 0 and "plain_arm" in wl:
+        p_ms, p_same = wl["plain_arm"](flush)
+        plain = {"ms": round(p_ms, 3), "equivalent_calls_per_s": round(stats_all[-1]["evals"] / (p_ms / 1e3), 1),
+                 "same_tallies": p_same,
+                 "what": "one thread per source photon walking its split descendants on a per-thread stack, "
+                         "one launch, best of 3; equivalent calls = the runtime's call count for these photons"}
+
     pk = peaks()
     s0 = stats_all[-1]
     alg = algorithmic_bytes(s0, wl["bytes_per_call"])
@@ -583,6 +615,7 @@ def main():
             "e2e": {"value": round(e2e_value, 1), "unit": "calls/s", "h2d_bytes_per_step": wl["h2d"],
                     "d2h_bytes_per_step": wl["d2h"]},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "plain_kernel": plain,
             "gpu_launches": wl["launches_per_step"] * args.steps,
             "runtime_stats": {"calls_per_step": s0["evals"], "full_batch_fraction": round(full, 4),
                               "spill_links": s0.get("spill_links"), "fill_links": s0.get("fill_links"),

@@ -112,6 +112,13 @@ struct LeanRings : BASE {
     };
 };
 
+// Tuning adapter: the spec compiled for at least MIN_CTAS resident CTAs per SM
+// (__launch_bounds__), which caps its registers.
+template <class BASE, size_t MIN_CTAS>
+struct MinCtas : BASE {
+    static const size_t MIN_CTAS_PER_SM = MIN_CTAS;
+};
+
 // Instantiates spec SPEC<RING, TEAMS> for the chosen program type and tuning variant.
 template <template <size_t, size_t> class SPEC, typename STATE>
 ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
@@ -124,6 +131,8 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_R2_T8: return new ProgramImpl<AsyncProgram<SPEC<2, 8>>>(arena, s);
             case HRM_VARIANT_LEAN_T2_M10: return new ProgramImpl<AsyncProgram<LeanRings<SPEC<4, 2>, 4, 2, 10>>>(arena, s);
             case HRM_VARIANT_LEAN_T2_M11: return new ProgramImpl<AsyncProgram<LeanRings<SPEC<4, 2>, 4, 2, 11>>>(arena, s);
+            case HRM_VARIANT_R4_T2_M9: return new ProgramImpl<AsyncProgram<MinCtas<SPEC<4, 2>, 9>>>(arena, s);
+            case HRM_VARIANT_R4_T4_M5: return new ProgramImpl<AsyncProgram<MinCtas<SPEC<4, 4>, 5>>>(arena, s);
             default: break;
         }
     } else if (type == HRM_EVENT) {
@@ -133,7 +142,9 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_R4_T2:
             case HRM_VARIANT_R8_T2:
             case HRM_VARIANT_LEAN_T2_M10:
-            case HRM_VARIANT_LEAN_T2_M11: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
+            case HRM_VARIANT_LEAN_T2_M11:
+            case HRM_VARIANT_R4_T2_M9: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
+            case HRM_VARIANT_R4_T4_M5: return new ProgramImpl<EventProgram<SPEC<2, 4>>>(arena, s);
             case HRM_VARIANT_R2_T8: return new ProgramImpl<EventProgram<SPEC<2, 8>>>(arena, s);
             default: break;
         }

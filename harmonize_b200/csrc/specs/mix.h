@@ -332,9 +332,9 @@ HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int 
 // The functions of each job kind form one ring group (RING_GROUP_OF): a kind never calls
 // another kind's functions, so a team holds promises of one kind at a time and the three
 // kinds' rings share one stash, as large as the photon rings alone. RING: ring links of the
-// photon functions (move and collide carry a whole photon, 12 words; every collide batch
-// feeds a batch of tallies, so each needs room for several batches); the Collatz and BFS
-// functions, with 5 words or fewer, get 2*RING links in the same space.
+// photon functions (a move carries a whole photon, 12 words with the job id, a collide 9;
+// every collide batch feeds a batch of tallies, so each needs room for several batches); the
+// Collatz and BFS functions, with 5 words or fewer, get 2*RING links in the same space.
 template <size_t RING = 4, size_t TEAMS = 4>
 struct MixSpec {
     typedef OpUnion<Job<CollatzEven>, Job<CollatzOdd>, Job<PhotonMove>, Job<PhotonCollide>, Job<PhotonTally>,

@@ -37,6 +37,16 @@ struct Photon {
     unsigned int voxel;
 };
 
+// A photon at a collision point. A collision redraws the direction, so a Collide promise
+// carries no direction: 8 argument words instead of the 11 of a moving photon.
+struct PhotonHit {
+    float x, y, z;
+    float w;
+    unsigned int id_lo, id_hi;
+    unsigned int step;
+    unsigned int voxel;
+};
+
 struct PhotonState {
     const float* mu_s;
     const float* absorb;
@@ -100,11 +110,17 @@ struct PhotonMove;
 struct PhotonCollide;
 struct PhotonTally;
 
+// A tally is one 64-bit word: the tally slot in bits 33-63 and the 2^-32 fixed-point amount
+// in bits 0-32 (an amount is at most 2^32: photon weights never exceed 1).
+HRM_HD HRM_FI unsigned long long tally_word(unsigned int slot, unsigned long long amount) {
+    return ((unsigned long long)slot << 33) | amount;
+}
+
 struct PhotonTally {
-    using Type = void (*)(unsigned int, unsigned long long);
+    using Type = void (*)(unsigned long long);
     template <typename PROGRAM>
-    HRM_DEV static void eval(PROGRAM prog, unsigned int slot, unsigned long long amount) {
-        hrm::atomic_add_u64(&prog.device.tally[slot], amount);
+    HRM_DEV static void eval(PROGRAM prog, unsigned long long t) {
+        hrm::atomic_add_u64(&prog.device.tally[t >> 33], t & 0x1FFFFFFFFull);
     }
 };
 
@@ -171,7 +187,8 @@ struct PhotonMove {
         p.y = hrm::fadd(p.y, hrm::fmul(t, p.dy));
         p.z = hrm::fadd(p.z, hrm::fmul(t, p.dz));
         if (collide) {
-            prog.template async<PhotonCollide>(p);
+            const PhotonHit h = {p.x, p.y, p.z, p.w, p.id_lo, p.id_hi, p.step, p.voxel};
+            prog.template async<PhotonCollide>(h);
             return;
         }
         // Land exactly on the face and step the voxel index along the crossing axis (written
@@ -186,7 +203,7 @@ struct PhotonMove {
         else if (axis == 1) { p.y = face; iy = c_next; }
         else { p.z = face; iz = c_next; }
         if (out) {
-            prog.template async<PhotonTally>(n * n * n + (p.id_lo & (PHOTON_SPREAD - 1u)), to_fixed(p.w));
+            prog.template async<PhotonTally>(tally_word(n * n * n + (p.id_lo & (PHOTON_SPREAD - 1u)), to_fixed(p.w)));
             return;
         }
         p.voxel = ix + n * (iy + n * iz);
@@ -213,28 +230,36 @@ struct PhotonMove {
 };
 
 struct PhotonCollide {
-    using Type = void (*)(Photon);
+    using Type = void (*)(PhotonHit);
     template <typename PROGRAM>
-    HRM_DEV static void eval(PROGRAM prog, Photon p) {
+    HRM_DEV static void eval(PROGRAM prog, PhotonHit h) {
         const PhotonState& s = prog.device;
         const unsigned int n = s.n;
-        float dep = hrm::fmul(p.w, s.absorb[p.voxel]);
-        p.w = hrm::fsub(p.w, dep);
-        prog.template async<PhotonTally>(p.voxel, to_fixed(dep));
-        if (p.w < WEIGHT_CUTOFF) {
+        float dep = hrm::fmul(h.w, s.absorb[h.voxel]);
+        float w = hrm::fsub(h.w, dep);
+        prog.template async<PhotonTally>(tally_word(h.voxel, to_fixed(dep)));
+        if (w < WEIGHT_CUTOFF) {
             // Russian roulette: a survivor tallies the weight it gains, a loser the weight it
             // loses (one call site for both, so that a warp of both kinds makes one call).
-            hrm::U32x4 r = photon_rng(s, p.id_lo, p.id_hi, p.step, PHASE_ROULETTE);
-            const unsigned int spread = p.id_lo & (PHOTON_SPREAD - 1u);
+            hrm::U32x4 r = photon_rng(s, h.id_lo, h.id_hi, h.step, PHASE_ROULETTE);
+            const unsigned int spread = h.id_lo & (PHOTON_SPREAD - 1u);
             const bool survive = hrm::u01_open0(r.x) <= ROULETTE_SURVIVAL;
-            const float boosted = hrm::fmul(p.w, ROULETTE_BOOST);
+            const float boosted = hrm::fmul(w, ROULETTE_BOOST);
             const unsigned int slot = n * n * n + (survive ? 2u : 1u) * PHOTON_SPREAD + spread;
-            prog.template async<PhotonTally>(slot, survive ? to_fixed(hrm::fsub(boosted, p.w)) : to_fixed(p.w));
+            prog.template async<PhotonTally>(tally_word(slot, survive ? to_fixed(hrm::fsub(boosted, w)) : to_fixed(w)));
             if (!survive) return;
-            p.w = boosted;
+            w = boosted;
         }
-        isotropic(s, p.id_lo, p.id_hi, p.step, p.dx, p.dy, p.dz);
-        p.step += 1u;
+        Photon p;
+        p.x = h.x;
+        p.y = h.y;
+        p.z = h.z;
+        p.w = w;
+        p.id_lo = h.id_lo;
+        p.id_hi = h.id_hi;
+        p.voxel = h.voxel;
+        isotropic(s, h.id_lo, h.id_hi, h.step, p.dx, p.dy, p.dz);
+        p.step = h.step + 1u;
         prog.template async<PhotonMove>(p);
     }
 };

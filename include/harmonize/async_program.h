@@ -200,8 +200,16 @@ class AsyncProgram {
         unsigned int active;       // ring group whose promises the stash holds, or NO_GROUP
         unsigned int held_n;       // overflow links written and not yet published
         unsigned int loads_pending;  // a lane issued cp.async copies of LazyLoad arguments
+        unsigned int overflowed;   // a push went past a ring since the last settle_overflow
         unsigned int held_e[HELD_MAX];  // their queue entries
         unsigned int held_f[HELD_MAX];  // their functions
+        // The team's statistics of this exec, kept here rather than in registers (lane 0
+        // updates them) and added to the device counters when the team leaves.
+        // n_batch_full: batches in bits 0-31, full batches in bits 32-63 (an exec runs at most
+        // one batch per cycle, and cycle counts are 32-bit); evaluations are counted per
+        // function in fn_evals.
+        unsigned long long n_batch_full, n_spill, n_fill, n_mw, n_idle;
+        unsigned long long fn_evals[FN];
         unsigned int words[RING_WORDS];
     };
 
@@ -571,6 +579,7 @@ class AsyncProgram {
         constexpr unsigned int W = Promise<TYPE>::WORDS;
         const unsigned int r = __popc(over & util::lanemask_lt());
         const unsigned int n = __popc(over);
+        if (r == 0) _grp_ctx.overflowed = 1u;
         unsigned int link = 0xFFFFFFFFu;
         unsigned int got = alloc_links_coop(1, r, over, link);
         link = __shfl_sync(over, link, __ffs(over) - 1);
@@ -718,11 +727,16 @@ class AsyncProgram {
         return nl;
     }
 
+    // Spills up to `nlinks` links of function f and counts them in the team's statistics.
     template <unsigned int I>
-    __device__ __forceinline__ void spill_fn(unsigned int f, unsigned int nlinks, unsigned long long& spilled) {
+    __device__ __forceinline__ void spill_fn(unsigned int f, unsigned int nlinks) {
         if constexpr (I < FN) {
-            if (f == I) spilled += spill_typed<I>(nlinks);
-            else spill_fn<I + 1>(f, nlinks, spilled);
+            if (f == I) {
+                const unsigned int nl = spill_typed<I>(nlinks);
+                if (util::lane_id() == 0) _grp_ctx.n_spill += nl;
+            } else {
+                spill_fn<I + 1>(f, nlinks);
+            }
         }
     }
 
@@ -824,6 +838,18 @@ class AsyncProgram {
         }
     }
 
+    // Whole team, after a batch: publishes the arena links of the promises that did not fit in
+    // the rings during the batch and clamps the counts. When no push overflowed (the common
+    // case) this is one shared-memory read.
+    __device__ __forceinline__ void settle_overflow() {
+        __syncwarp();
+        if (*(volatile unsigned int*)&_grp_ctx.overflowed == 0u) return;
+        __syncwarp();
+        if (util::lane_id() == 0) _grp_ctx.overflowed = 0u;
+        publish_held();
+        clamp_counts();
+    }
+
     // Counts above the ring size mean the excess went to the arena: clamp.
     __device__ __forceinline__ void clamp_counts() {
         __syncwarp();
@@ -874,11 +900,18 @@ class AsyncProgram {
         if (lane < FN) {
             _grp_ctx.count[lane] = 0;
             _grp_ctx.bottom[lane] = 0;
+            _grp_ctx.fn_evals[lane] = 0;
         }
         if (lane == 0) {
             _grp_ctx.active = NO_GROUP;
             _grp_ctx.held_n = 0;
             _grp_ctx.loads_pending = 0;
+            _grp_ctx.overflowed = 0;
+            _grp_ctx.n_batch_full = 0;
+            _grp_ctx.n_spill = 0;
+            _grp_ctx.n_fill = 0;
+            _grp_ctx.n_mw = 0;
+            _grp_ctx.n_idle = 0;
         }
         __syncwarp();
     }
@@ -898,8 +931,6 @@ class AsyncProgram {
         bool can_make_work = true;
         bool counted_idle = false;
         unsigned int backoff = 32;
-        unsigned long long n_evals = 0, n_batches = 0, n_full = 0, n_spill = 0, n_fill = 0, n_mw = 0, n_idle = 0;
-        unsigned long long fn_evals = 0;  // lane f counts the evaluations of function f
         unsigned int prev_c = 0;          // lane f: f's count at the previous step
         unsigned int age = 0;             // lane f: steps f has held a partial batch that did not grow
         unsigned int rotate = 0;          // next function to favour for a forced partial batch
@@ -973,7 +1004,7 @@ class AsyncProgram {
                         __syncwarp();
                         for (unsigned int f = 0; f < FN; f++) {
                             unsigned int cf = g.count[f];
-                            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
+                            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u);
                         }
                         if (__all_sync(0xFFFFFFFFu, lane >= FN || g.count[lane] == 0u)) continue;
                     }
@@ -989,7 +1020,7 @@ class AsyncProgram {
                         __syncwarp();
                     }
                     unsigned int took = fill_fn<0>(ff);
-                    n_fill += took;
+                    if (lane == 0) g.n_fill += took;
                     if (took > 0) continue;
                     // Another team won the race for that work. Never make new work while
                     // the arena holds a backlog: run what is local, or look again.
@@ -1006,7 +1037,7 @@ class AsyncProgram {
                     bool more = hrm_rt::call_make_work<PROGRAM_SPEC>(*this);
                     publish_held();
                     can_make_work = __any_sync(0xFFFFFFFFu, more);
-                    n_mw++;
+                    if (lane == 0) g.n_mw++;
                     clamp_counts();
                     const unsigned int after = __reduce_add_sync(0xFFFFFFFFu, (lane < FN) ? g.count[lane] : 0u);
                     // New local work: plan again. Nothing local at all: keep asking. Otherwise
@@ -1023,7 +1054,7 @@ class AsyncProgram {
                     if (lane == 0) st = idle_poll(counted_idle, backoff);
                     st = __shfl_sync(0xFFFFFFFFu, st, 0);
                     counted_idle = __shfl_sync(0xFFFFFFFFu, (unsigned int)counted_idle, 0) != 0;
-                    n_idle++;
+                    if (lane == 0) g.n_idle++;
                     if (st == 2) { quiescent = true; break; }
                     continue;
                 }
@@ -1047,16 +1078,15 @@ class AsyncProgram {
                 hi &= hi - 1;
                 unsigned int cf = __shfl_sync(0xFFFFFFFFu, c, f);
                 unsigned int rf = __shfl_sync(0xFFFFFFFFu, my_ring, f);
-                spill_fn<0>(f, (cf - (rf - 32u) + 31u) / 32u, n_spill);
+                spill_fn<0>(f, (cf - (rf - 32u) + 31u) / 32u);
             }
             run_fn<0>(bf, k);
             hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
-            publish_held();
-            clamp_counts();
-            n_evals += k;
-            n_batches += 1;
-            n_full += (k == 32u);
-            if (lane == bf) fn_evals += k;
+            settle_overflow();
+            if (lane == 0) {
+                g.n_batch_full += 1ull + ((unsigned long long)(k == 32u) << 32);
+                g.fn_evals[bf] += k;
+            }
         }
 
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
@@ -1068,9 +1098,14 @@ class AsyncProgram {
         // Leave nothing in shared memory: spill every pending promise.
         for (unsigned int f = 0; f < FN; f++) {
             unsigned int cf = g.count[f];
-            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u, n_spill);
+            if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u);
         }
-        if (lane < FN && fn_evals != 0) atomicAdd(&_dev_ctx.stats[hrm_rt::STAT_FN_EVALS + lane], fn_evals);
+        __syncwarp();
+        const unsigned long long my_evals = (lane < FN) ? g.fn_evals[lane] : 0ull;
+        if (my_evals != 0) atomicAdd(&_dev_ctx.stats[hrm_rt::STAT_FN_EVALS + lane], my_evals);
+        unsigned long long n_evals = my_evals;
+#pragma unroll
+        for (unsigned int o = 16; o > 0; o >>= 1) n_evals += __shfl_xor_sync(0xFFFFFFFFu, n_evals, o);
         if (lane == 0) {
             if (can_make_work) atomicOr(&ctl->flags, EARLY_HALT_FLAG);
             for (unsigned int f = 0; f < FN; f++) {
@@ -1082,12 +1117,12 @@ class AsyncProgram {
             }
             unsigned long long* st = _dev_ctx.stats;
             atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);
-            atomicAdd(&st[hrm_rt::STAT_BATCHES], n_batches);
-            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], n_full);
-            atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], n_spill);
-            atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], n_fill);
-            atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], n_mw);
-            atomicAdd(&st[hrm_rt::STAT_IDLE_POLLS], n_idle);
+            atomicAdd(&st[hrm_rt::STAT_BATCHES], g.n_batch_full & 0xFFFFFFFFull);
+            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_batch_full >> 32);
+            atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], g.n_spill);
+            atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], g.n_fill);
+            atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], g.n_mw);
+            atomicAdd(&st[hrm_rt::STAT_IDLE_POLLS], g.n_idle);
             (void)quiescent;
             __threadfence();
             unsigned int out = atomicAdd(&ctl->checkout, 1u);

@@ -160,6 +160,66 @@ struct OpType<RETURN (*)(ARGS...)> {
 };
 
 // ---------------------------------------------------------------------------------------
+// Packed argument words: the runtime moves a promise as 32-bit words with its arguments laid
+// end to end in call order, each rounded up to whole words and with no alignment padding
+// between them (a (uint32, uint64) call is 3 words, not the 4 of its ArgTuple).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr unsigned int words_of() {
+    return (unsigned int)((sizeof(T) + 3) / 4);
+}
+
+template <typename TUPLE>
+struct ArgWords;
+
+template <>
+struct ArgWords<ArgTuple<>> {
+    static const unsigned int COUNT = 0;
+    template <unsigned int O, unsigned int N>
+    __host__ __device__ static void put(const ArgTuple<>&, unsigned int (&)[N]) {}
+    template <unsigned int O, unsigned int N>
+    __host__ __device__ static void get(ArgTuple<>&, const unsigned int (&)[N]) {}
+};
+
+template <typename HEAD, typename... TAIL>
+struct ArgWords<ArgTuple<HEAD, TAIL...>> {
+    using Rest = ArgWords<ArgTuple<TAIL...>>;
+    static const unsigned int HEAD_WORDS = words_of<HEAD>();
+    static const unsigned int COUNT = HEAD_WORDS + Rest::COUNT;
+    // Writes the arguments to words [O, O + COUNT) of w.
+    template <unsigned int O, unsigned int N>
+    __host__ __device__ static void put(const ArgTuple<HEAD, TAIL...>& t, unsigned int (&w)[N]) {
+        unsigned int tmp[HEAD_WORDS];
+        tmp[HEAD_WORDS - 1] = 0u;
+        memcpy(tmp, &t.head, sizeof(HEAD));
+#pragma unroll
+        for (unsigned int i = 0; i < HEAD_WORDS; i++) w[O + i] = tmp[i];
+        Rest::template put<O + HEAD_WORDS>(t, w);
+    }
+    // Reads the arguments back from words [O, O + COUNT) of w.
+    template <unsigned int O, unsigned int N>
+    __host__ __device__ static void get(ArgTuple<HEAD, TAIL...>& t, const unsigned int (&w)[N]) {
+        unsigned int tmp[HEAD_WORDS];
+#pragma unroll
+        for (unsigned int i = 0; i < HEAD_WORDS; i++) tmp[i] = w[O + i];
+        memcpy(&t.head, tmp, sizeof(HEAD));
+        Rest::template get<O + HEAD_WORDS>(t, w);
+    }
+};
+
+// First word of argument I in the packed words.
+template <size_t I, typename TUPLE>
+struct ArgWordOffset;
+template <typename HEAD, typename... TAIL>
+struct ArgWordOffset<0, ArgTuple<HEAD, TAIL...>> {
+    static const unsigned int value = 0;
+};
+template <size_t I, typename HEAD, typename... TAIL>
+struct ArgWordOffset<I, ArgTuple<HEAD, TAIL...>> {
+    static const unsigned int value = words_of<HEAD>() + ArgWordOffset<I - 1, ArgTuple<TAIL...>>::value;
+};
+
+// ---------------------------------------------------------------------------------------
 // Promise<Op>: the arguments of one call to Op.
 // ---------------------------------------------------------------------------------------
 template <typename OPERATION>
@@ -170,8 +230,9 @@ struct Promise {
 
     Args args;
 
-    // Number of 32-bit words the runtime moves for this promise.
-    static const unsigned int WORDS = (unsigned int)((sizeof(Args) + 3) / 4);
+    // Number of 32-bit words the runtime moves for this promise (packed, see ArgWords; at
+    // least one).
+    static const unsigned int WORDS = ArgWords<Args>::COUNT ? ArgWords<Args>::COUNT : 1u;
 
     Promise() = default;
     template <typename... ARGS>
@@ -190,10 +251,10 @@ struct Promise {
     // Word-level access used by the runtime's queues.
     __device__ __forceinline__ void to_words(unsigned int (&w)[WORDS]) const {
         w[WORDS - 1] = 0u;
-        memcpy(w, &args, sizeof(Args));
+        ArgWords<Args>::template put<0>(args, w);
     }
     __device__ __forceinline__ void from_words(const unsigned int (&w)[WORDS]) {
-        memcpy(&args, w, sizeof(Args));
+        ArgWords<Args>::template get<0>(args, w);
     }
 };
 

@@ -420,12 +420,13 @@ __device__ __forceinline__ void mark_lazy_words(ARGS& tuple, bool* lazy, const u
                                                 TAIL... tail) {
     if constexpr (is_lazy_load<HEAD>::value) {
         using T = typename HEAD::Type;
-        const size_t off = (size_t)((const char*)&TupleGet<I, ARGS>::get(tuple) - (const char*)&tuple);
+        constexpr unsigned int off = ArgWordOffset<I, ARGS>::value;  // packed word of argument I
         const unsigned int* from = (const unsigned int*)&head.reference;
+        (void)tuple;
 #pragma unroll
         for (unsigned int j = 0; j < sizeof(T) / 4u; j++) {
-            lazy[off / 4u + j] = true;
-            src[off / 4u + j] = from + j;
+            lazy[off + j] = true;
+            src[off + j] = from + j;
         }
     }
     mark_lazy_words<ARGS, I + 1>(tuple, lazy, src, tail...);
