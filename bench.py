@@ -214,8 +214,8 @@ def flush_l2(buf):
 # ---------------------------------------------------------------------------------------
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one exec launch on a
 # small case of the same kernel, with its call count: scaled by calls to the bench's launch
-# (profiles/photon_walk_async_exec_kernel_ncu.txt: 10^5 photons, variant R4/T2).
-TRAFFIC_PROFILE = {("photon", "async"): (2631936 + 375808, 161486336)}
+# (profiles/photon_walk_async_exec_kernel_ncu.txt: 10^6 photons, variant 7).
+TRAFFIC_PROFILE = {("photon", "async"): (50077184 + 650106112, 1613907450)}
 
 BYTES_PER_CALL = {
     "photon": [93, 68, 32],
@@ -585,7 +585,7 @@ def main():
     traffic = round(prof[0] / prof[1] * s0["evals"]) if prof else None
     roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": traffic,
-                "traffic_source": ("ncu DRAM bytes of a 10^5-photon launch scaled by calls" if prof else None),
+                "traffic_source": ("ncu DRAM bytes of a 10^6-photon launch scaled by calls" if prof else None),
                 "peak_source": pk["source"],
                 "algorithmic_bytes_per_launch": alg,
                 "note": "algorithmic bytes = each call's promise written and read once plus its compulsory "

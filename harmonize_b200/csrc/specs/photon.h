@@ -389,6 +389,13 @@ struct PhotonSpec {
     static const size_t POOL_SIZE = 16069;
     static const size_t RING_LINKS = RING;
     static const size_t TEAMS_PER_CTA = TEAMS;
+    // Collide has half the ring links of the others (at least 2): a batch of moves makes at
+    // most one collide per lane, so two links always hold a batch's calls, and the smaller
+    // stash leaves room for more teams per SM (R4/T2: 12 CTAs instead of 10).
+    template <typename Op>
+    struct RING_LINKS_OF {
+        static const size_t value = std::is_same<Op, PhotonCollide>::value ? (RING / 2 < 2 ? 2 : RING / 2) : RING;
+    };
 
     template <typename PROGRAM>
     HRM_DEV static void initialize(PROGRAM) {}

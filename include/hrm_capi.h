@@ -104,10 +104,10 @@ typedef struct hrm_run_config {
  * for at least 10 (M10) or 11 (M11) resident CTAs per SM (more teams per SM, fewer registers). */
 #define HRM_VARIANT_LEAN_T2_M10 5
 #define HRM_VARIANT_LEAN_T2_M11 6
-/* 4-link rings, 2 teams per CTA, compiled for at least 9 resident CTAs per SM; 4-link rings,
+/* 4-link rings, 2 teams per CTA, compiled for at least 11 resident CTAs per SM; 4-link rings,
  * 4 teams per CTA, at least 5 CTAs per SM (register caps that leave shared memory the only
  * limit on teams per SM). */
-#define HRM_VARIANT_R4_T2_M9 7
+#define HRM_VARIANT_R4_T2_M11 7
 #define HRM_VARIANT_R4_T4_M5 8
 #define HRM_VARIANT_COUNT 9
 

@@ -23,7 +23,10 @@ static_assert(fn_OLDEST_FIRST<BfsSpec<2, 8>, BfsRelax>::value && fn_OLDEST_FIRST
               "BFS functions oldest first");
 static_assert(!fn_OLDEST_FIRST<PhotonSpec<4, 2>, PhotonMove>::value, "photon newest first");
 static_assert(!fn_OLDEST_FIRST<CollatzSpec<>, CollatzOdd>::value, "Collatz newest first");
-static_assert(fn_RING_LINKS<PhotonSpec<4, 2>, PhotonTally>::value == 4, "no RING_LINKS_OF: RING_LINKS");
+static_assert(fn_RING_LINKS<CollatzSpec<4, 2>, CollatzOdd>::value == 4, "no RING_LINKS_OF: RING_LINKS");
+static_assert(fn_RING_LINKS<PhotonSpec<4, 2>, PhotonTally>::value == 4, "RING_LINKS_OF: RING_LINKS for the others");
+static_assert(fn_RING_LINKS<PhotonSpec<4, 2>, PhotonCollide>::value == 2, "RING_LINKS_OF: collide half");
+static_assert(fn_RING_LINKS<PhotonSpec<2, 4>, PhotonCollide>::value == 2, "RING_LINKS_OF: at least 2 links");
 static_assert(fn_RING_GROUP<PhotonSpec<4, 2>, PhotonMove>::value == 0, "no RING_GROUP_OF: one group");
 
 // Per function, the job-multiplexing spec: groups by job kind, photon rings RING links and

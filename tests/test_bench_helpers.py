@@ -35,7 +35,7 @@ def test_latency_percentiles_in_ms():
 
 def test_algorithmic_bytes_weight_each_function_by_its_bytes():
     stats = {"fn0_evals": 10, "fn1_evals": 5, "fn2_evals": 2}
-    assert bench.algorithmic_bytes(stats, bench.BYTES_PER_CALL["photon"]) == 10 * 93 + 5 * 92 + 2 * 48
+    assert bench.algorithmic_bytes(stats, bench.BYTES_PER_CALL["photon"]) == 10 * 93 + 5 * 68 + 2 * 32
     assert bench.algorithmic_bytes({}, [32, 32]) == 0
 
 
