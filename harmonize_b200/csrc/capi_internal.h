@@ -15,9 +15,24 @@ namespace hrm_capi {
 // Records `msg` as the calling thread's last error (read by hrm_last_error) and returns code.
 int set_error(int code, const std::string& msg);
 
-// Teams (32-lane work groups) of the single-spec photon-walk AsyncProgram of tuning variant
-// `variant` that can be resident on one SM of the current device at once.
-unsigned int photon_teams_per_sm(int variant);
+// What one CTA of a persistent exec kernel holds on an SM: registers per thread, threads and
+// shared memory (static + dynamic) per CTA.
+struct CtaFootprint {
+    unsigned int regs_per_thread = 0;
+    unsigned int threads = 0;
+    size_t smem = 0;
+};
+
+// The CTA footprint of the single-spec photon-walk AsyncProgram exec kernel of tuning variant
+// `variant` on the current device (HRM_VARIANT_R4_T4_M5 only).
+CtaFootprint photon_cta_footprint(int variant);
+
+// CTAs per SM of kernel B that fit beside `a_ctas` CTAs per SM of kernel A on the current
+// device: shared memory (with the per-CTA reservation), threads, CTA slots, and registers per
+// SM sub-partition (a quarter of the register file; a CTA's warps spread over the four
+// sub-partitions, so a kernel of w warps per CTA at c CTAs takes ceil(c*w/4) warps' registers
+// from each).
+unsigned int ctas_beside(const CtaFootprint& a, unsigned int a_ctas, const CtaFootprint& b);
 
 // Two timing events, destroyed on every path out of the scope that made them (a failed
 // launch or a device error flag throws between record and read).

@@ -17,6 +17,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstddef>
 #include <deque>
@@ -123,28 +126,6 @@ __global__ void stamp_kernel(unsigned long long* t) {
     if (threadIdx.x == 0) *t = hrm_specs::global_ns();
 }
 
-// Completion stamp of a job served outside the persistent kernel, into the host-mapped array.
-__global__ void stamp_done_kernel(unsigned long long* done, unsigned int j) {
-    if (threadIdx.x == 0) {
-        volatile unsigned long long* d = done;
-        d[j] = hrm_specs::global_ns();
-        __threadfence_system();
-    }
-}
-
-// Clears the outputs of jobs [first, first+n) before they are published to a running kernel.
-__global__ void mix_prepare_range_kernel(JobRecord* jobs, unsigned int first, unsigned int n) {
-    for (unsigned int j = first + blockIdx.x; j < first + n; j += gridDim.x) {
-        JobRecord& r = jobs[j];
-        if (r.kind == hrm_specs::JOB_PHOTON) {
-            size_t slots = (size_t)r.s.p.n * r.s.p.n * r.s.p.n + 3u * hrm_specs::PHOTON_SPREAD;
-            for (size_t i = threadIdx.x; i < slots; i += blockDim.x) r.s.p.tally[i] = 0ull;
-        } else if (r.kind == hrm_specs::JOB_BFS) {
-            for (size_t i = threadIdx.x; i < r.s.b.nv; i += blockDim.x) r.s.b.levels[i] = 0xFFFFFFFFu;
-        }
-    }
-}
-
 // The order in which make_work serves jobs (hrm_run_config.job_order).
 unsigned int job_order_of(const hrm_run_config& cfg) {
     switch (cfg.job_order) {
@@ -153,11 +134,6 @@ unsigned int job_order_of(const hrm_run_config& cfg) {
         case HRM_JOB_ORDER_SMALL_FIRST: return hrm_specs::JOB_ORDER_SMALL_FIRST;
         default: throw std::invalid_argument("unknown job_order");
     }
-}
-
-// Asks a running exec to stop (the same request prog.halt_early() makes).
-__global__ void halt_kernel(hrm_rt::RuntimeControl* ctl) {
-    if (threadIdx.x == 0) atomicOr(&ctl->flags, hrm_rt::EARLY_HALT_FLAG);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -383,7 +359,29 @@ __global__ void __launch_bounds__(1024) bfs_plain_block_kernel(const unsigned in
 // ---------------------------------------------------------------------------------------
 // Serving: a resident runtime that admits jobs while it runs.
 // ---------------------------------------------------------------------------------------
+// Session trace: with HRM_SERVE_TRACE set in the environment, a serving session writes one
+// line per event (exec launched and ended, solo job started and ended, halt requested,
+// admission held back) to stderr, stamped in milliseconds since the session opened.
+struct SessionTrace {
+    const bool on = std::getenv("HRM_SERVE_TRACE") != nullptr;
+    const std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    std::mutex lock;
+    void operator()(const char* fmt, ...) {
+        if (!on) return;
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::lock_guard<std::mutex> g(lock);
+        std::fprintf(stderr, "[hrm serve %10.3f ms] ", ms);
+        va_list ap;
+        va_start(ap, fmt);
+        std::vfprintf(stderr, fmt, ap);
+        va_end(ap);
+        std::fputc('\n', stderr);
+    }
+};
+
 struct ServerBase {
+    SessionTrace trace;
     virtual ~ServerBase() {}
     virtual unsigned int submit(const hrm_job* jobs, unsigned int n) = 0;  // returns first index
     virtual unsigned int poll(uint64_t* done_ns, unsigned int max) = 0;    // returns completed count
@@ -404,7 +402,14 @@ struct Server : ServerBase {
     util::host::DevBuf<unsigned int> counters;  // admitted, cursor, open, completed, closed
     unsigned long long* done_host = nullptr;    // mapped: %globaltimer of completion per job
     JobRecord* staging = nullptr;               // pinned staging for job records
-    unsigned int* pinned_ctr = nullptr;         // pinned staging for counter writes
+    unsigned int* pinned_ctr = nullptr;         // pinned staging for counter writes; [6] = 1, [7] = 0
+    // Pinned fill patterns (all zero bytes, all 0xFF bytes) that the copy engine writes over a
+    // submitted job's outputs: while the persistent kernel holds every SM, a kernel launched
+    // to clear them would wait for the exec to end.
+    static const size_t PATTERN_BYTES = (size_t)1 << 20;
+    unsigned char* zeros = nullptr;
+    unsigned char* ones = nullptr;
+    long long clock_offset_ns = 0;              // %globaltimer - host steady clock, at set-up
     unsigned int capacity;
     std::atomic<unsigned int> submitted{0};  // written by submit, read by poll and close
     size_t groups, cycles;
@@ -419,24 +424,27 @@ struct Server : ServerBase {
     // Solo lane, partitioned residency: photon jobs of at least solo_photons photons fill the
     // GPU on their own and run at about half speed inside the multiplexing kernel, so the
     // session serves them through the single-spec runtime, BESIDE the resident kernel: while
-    // a solo job is queued or running, the resident kernel is launched with half of its teams
-    // per SM (half_groups) and the solo job's kernel with half of its own (solo_groups), so
-    // both are resident at once and the small jobs keep flowing. With no solo work the
-    // resident kernel runs with all its teams. submit queues a solo job and, if the resident
+    // a solo job is queued or running, the resident kernel is launched with a quarter of its
+    // CTAs per SM (shared_groups) and the solo job's kernel with as many CTAs per SM as fit beside
+    // them (solo_groups; shared memory, threads, and registers per SM sub-partition), so both
+    // are resident at once and the small jobs keep flowing. With no solo work the resident
+    // kernel runs with all its teams. submit queues a solo job and, if the resident
     // exec on the GPU holds every team, halts it (teams spill their work and leave within a
-    // few scheduling rounds) so that the runner relaunches it with half; the solo runner
-    // halts the half-share exec once the queue drains, so that it comes back with all teams.
+    // few scheduling rounds) so that the runner relaunches it with its share; the solo runner
+    // halts the shared exec once the queue drains, so that it comes back with all teams.
     // A solo job's record is a placeholder with an empty source, which the kernel closes and
     // never works on; its completion is stamped by the solo runner.
     unsigned int solo_photons;
+    // The solo lane's photon kernel: 4 teams per CTA (one warp per SM sub-partition).
+    static const int SOLO_VARIANT = HRM_VARIANT_R4_T4_M5;
     std::mutex solo_lock;                                     // guards the fields below
     std::condition_variable solo_cv;
     std::deque<std::pair<unsigned int, hrm_job>> solo_queue;  // (job index, job)
     bool solo_running = false;                                // a solo job is on the GPU
-    bool exec_half = false;                                   // the exec on the GPU holds half the teams
+    bool exec_shared = false;                                   // the exec on the GPU holds its share beside the solo lane
     bool exec_on_gpu = false;                                 // a resident exec is launched
     bool solo_exit = false;                                   // the solo runner should stop
-    size_t half_groups = 0, solo_groups = 0;
+    size_t shared_groups = 0, solo_groups = 0;
     cudaStream_t solo_s = nullptr;
     std::thread solo_runner;
     unsigned long long* done_dev = nullptr;                    // device alias of done_host
@@ -466,6 +474,12 @@ struct Server : ServerBase {
         ck(cudaHostGetDevicePointer((void**)&done_dev, done_host, 0), "done flags device alias");
         ck(cudaHostAlloc((void**)&staging, sizeof(JobRecord) * 4096, cudaHostAllocDefault), "staging");
         ck(cudaHostAlloc((void**)&pinned_ctr, sizeof(unsigned int) * 8, cudaHostAllocDefault), "staging");
+        memset(pinned_ctr, 0, sizeof(unsigned int) * 8);
+        pinned_ctr[6] = 1u;
+        ck(cudaHostAlloc((void**)&zeros, PATTERN_BYTES, cudaHostAllocDefault), "fill pattern");
+        ck(cudaHostAlloc((void**)&ones, PATTERN_BYTES, cudaHostAllocDefault), "fill pattern");
+        memset(zeros, 0, PATTERN_BYTES);
+        memset(ones, 0xFF, PATTERN_BYTES);
         ck(cudaStreamCreateWithFlags(&exec_s, cudaStreamNonBlocking), "stream");
         ck(cudaStreamCreateWithFlags(&submit_s, cudaStreamNonBlocking), "stream");
         MixState st = Batch<P>::state_for(jobs.data(), counters.data(), cap);
@@ -478,44 +492,67 @@ struct Server : ServerBase {
         ck(cudaMemcpy(counters.data(), ctr, sizeof(ctr), cudaMemcpyHostToDevice), "counters");
         P::launch_init(inst, groups, exec_s);
         ck(cudaStreamSynchronize(exec_s), "init");
-        // Load the kernels that the session launches while its persistent kernel runs. A
-        // kernel loaded on first use (lazy module loading) cannot start until the running
-        // persistent kernel ends, which held the first jobs of a session back by one whole
-        // exec (seconds).
-        cudaFuncAttributes fa;
-        ck(cudaFuncGetAttributes(&fa, mix_prepare_range_kernel), "kernel load");
-        ck(cudaFuncGetAttributes(&fa, halt_kernel), "kernel load");
-        ck(cudaFuncGetAttributes(&fa, stamp_done_kernel), "kernel load");
-        mix_prepare_range_kernel<<<1, 32, 0, submit_s>>>(jobs.data(), 0u, 0u);
-        ck(cudaGetLastError(), "kernel load");
-        ck(cudaStreamSynchronize(submit_s), "kernel load");
+        // While the persistent kernel runs, the session launches no kernel of its own (a
+        // kernel needs room on an SM, which the persistent kernel may leave none of): job
+        // outputs are cleared and halts requested by copies, and solo completions stamped by
+        // the host in %globaltimer units through this offset (one probe, before the session).
+        {
+            util::host::DevBuf<unsigned long long> probe((size_t)1);
+            const auto h0 = std::chrono::steady_clock::now();
+            stamp_kernel<<<1, 32, 0, submit_s>>>(probe.data());
+            ck(cudaGetLastError(), "clock probe");
+            ck(cudaStreamSynchronize(submit_s), "clock probe");
+            const auto h1 = std::chrono::steady_clock::now();
+            unsigned long long g = 0;
+            ck(cudaMemcpy(&g, probe.data(), sizeof(g), cudaMemcpyDeviceToHost), "clock probe");
+            const long long mid = std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                      (h0 + (h1 - h0) / 2).time_since_epoch()).count();
+            clock_offset_ns = (long long)g - mid;
+        }
         if (solo_photons) {
             // Half of each kernel's resident teams per SM: two halves fit one SM together.
             ck(cudaStreamCreateWithFlags(&solo_s, cudaStreamNonBlocking), "stream");
             int dev = 0, sms = 1;
             ck(cudaGetDevice(&dev), "cudaGetDevice");
             ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+            // A quarter of the resident kernel's CTAs per SM, and as many CTAs of the solo photon
+            // kernel (4 teams per CTA, so that each CTA puts one warp on each SM sub-partition)
+            // as fit beside them; fewer resident CTAs if none fit. Large photon jobs carry most
+            // of the mix's work, so the solo lane gets the larger share: with half each, the
+            // lane saturated at 0.75 of the plain kernels' job rate.
             const unsigned int mix_ctas_per_sm = P::resident_ctas() / (unsigned int)sms;
-            const unsigned int solo_teams_per_sm = hrm_capi::photon_teams_per_sm(HRM_VARIANT_R4_T2);
-            half_groups = (size_t)std::max(1u, mix_ctas_per_sm / 2u) * (size_t)sms * P::TEAMS_PER_CTA;
-            solo_groups = (size_t)std::max(2u, (solo_teams_per_sm / 2u) & ~1u) * (size_t)sms;
-            // The solo job's kernel must start before the half-share exec may be counted on:
+            cudaFuncAttributes mf;
+            ck(cudaFuncGetAttributes(&mf, hrm_rt::async_exec_kernel<P>), "kernel attributes");
+            hrm_capi::CtaFootprint mix_cta;
+            mix_cta.regs_per_thread = (unsigned int)mf.numRegs;
+            mix_cta.threads = P::CTA_THREADS;
+            mix_cta.smem = mf.sharedSizeBytes + P::SMEM_BYTES;
+            const hrm_capi::CtaFootprint solo_cta = hrm_capi::photon_cta_footprint(SOLO_VARIANT);
+            unsigned int m = std::max(1u, mix_ctas_per_sm / 4u), s = 0;
+            while (m > 0 && (s = hrm_capi::ctas_beside(mix_cta, m, solo_cta)) == 0) m--;
+            if (m == 0 || s == 0) throw std::runtime_error("solo lane: the photon kernel fits beside no resident CTA");
+            shared_groups = (size_t)m * (size_t)sms * P::TEAMS_PER_CTA;
+            solo_groups = (size_t)s * (size_t)sms * (solo_cta.threads / 32u);
+            trace("solo lane: resident %u of %u CTAs per SM (%u regs, %zu B), solo photon %u CTAs per SM "
+                  "(%u regs, %zu B): shared_groups %zu solo_groups %zu",
+                  m, mix_ctas_per_sm, mix_cta.regs_per_thread, mix_cta.smem, s, solo_cta.regs_per_thread,
+                  solo_cta.smem, shared_groups, solo_groups);
+            // The solo job's kernel must start before the shared exec may be counted on:
             // load it now (lazy loading would hold it back until a running kernel ends).
             hrm_run_config c;
             memset(&c, 0, sizeof(c));
             c.program_type = HRM_ASYNC;
-            c.variant = HRM_VARIANT_R4_T2;
+            c.variant = SOLO_VARIANT;
             c.stream = solo_s;
             c.groups = solo_groups;
-            util::host::DevBuf<float> m((size_t)8);
+            util::host::DevBuf<float> mu((size_t)8);
             util::host::DevBuf<unsigned char> sp((size_t)8);
             util::host::DevBuf<unsigned long long> t((size_t)(8 + 3 * hrm_specs::PHOTON_SPREAD));
-            ck(cudaMemset(m.data(), 0, 8 * sizeof(float)), "warm-up medium");
+            ck(cudaMemset(mu.data(), 0, 8 * sizeof(float)), "warm-up medium");
             ck(cudaMemset(sp.data(), 0, 8), "warm-up medium");
             hrm_run_result r;
-            if (hrm_photon_run_device(m.data(), m.data(), sp.data(), 2, 1, 0, 0, (uint64_t*)t.data(), &c, &r) != HRM_OK)
+            if (hrm_photon_run_device(mu.data(), mu.data(), sp.data(), 2, 1, 0, 0, (uint64_t*)t.data(), &c, &r) != HRM_OK)
                 throw std::runtime_error(std::string("solo lane warm-up: ") + hrm_last_error());
-            ck(cudaFuncGetAttributes(&fa, stamp_done_kernel), "kernel load");
         }
     }
 
@@ -527,10 +564,13 @@ struct Server : ServerBase {
         if (done_host) cudaFreeHost(done_host);
         if (staging) cudaFreeHost(staging);
         if (pinned_ctr) cudaFreeHost(pinned_ctr);
+        if (zeros) cudaFreeHost(zeros);
+        if (ones) cudaFreeHost(ones);
         exec_s = submit_s = nullptr;
         done_host = nullptr;
         staging = nullptr;
         pinned_ctr = nullptr;
+        zeros = ones = nullptr;
     }
 
     // Teardown is bounded: the session is closed, the running exec is asked to halt (teams
@@ -542,7 +582,7 @@ struct Server : ServerBase {
         if (runner.joinable()) {
             pinned_ctr[2] = 0;
             cudaMemcpyAsync(counters.data() + 2, pinned_ctr + 2, 4, cudaMemcpyHostToDevice, submit_s);
-            halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
+            cudaMemcpyAsync(&inst.control.data()->halt_request, pinned_ctr + 6, 4, cudaMemcpyHostToDevice, submit_s);
             cudaStreamSynchronize(submit_s);
             runner.join();
         }
@@ -560,30 +600,35 @@ struct Server : ServerBase {
     }
 
     void halt_resident() {
-        halt_kernel<<<1, 32, 0, submit_s>>>(inst.control.data());
-        ck(cudaGetLastError(), "halt");
+        trace("halt requested");
+        ck(cudaMemcpyAsync(&inst.control.data()->halt_request, pinned_ctr + 6, 4, cudaMemcpyHostToDevice, submit_s),
+           "halt");
         ck(cudaStreamSynchronize(submit_s), "halt");
     }
 
-    // One solo job on the solo stream, beside the half-share resident exec.
+    // One solo job on the solo stream, beside the shared resident exec.
     void run_solo(unsigned int j, const hrm_job& jb) {
         hrm_run_config c;
         memset(&c, 0, sizeof(c));
         c.program_type = HRM_ASYNC;
-        c.variant = HRM_VARIANT_R4_T2;  // the photon walk's tuned variant on this GPU
+        c.variant = SOLO_VARIANT;
         c.stream = solo_s;
         c.groups = solo_groups;
         hrm_run_result r;
+        trace("solo job %u (%u photons) starts", j, jb.count);
         if (hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
                                   jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
             throw std::runtime_error(std::string("solo photon job: ") + hrm_last_error());
-        stamp_done_kernel<<<1, 32, 0, solo_s>>>(done_dev, j);
-        ck(cudaGetLastError(), "solo stamp");
-        ck(cudaStreamSynchronize(solo_s), "solo stamp");
+        trace("solo job %u ends: %.3f ms on the device, %u execs", j, r.device_ms, r.execs);
+        // The run above synchronised with its stream: stamp the completion from the host.
+        const long long now = std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                  std::chrono::steady_clock::now().time_since_epoch()).count();
+        const unsigned long long stamp = (unsigned long long)(now + clock_offset_ns);
+        ((volatile unsigned long long*)done_host)[j] = stamp ? stamp : 1ull;
     }
 
     // The solo runner: serves the solo queue in submission order, one job at a time, only
-    // while the resident exec holds half of its teams (or no resident exec is running).
+    // while the resident exec holds only its share (or no resident exec is running).
     void solo_loop() {
         try {
             while (true) {
@@ -591,10 +636,10 @@ struct Server : ServerBase {
                 {
                     std::unique_lock<std::mutex> g(solo_lock);
                     solo_cv.wait_for(g, std::chrono::milliseconds(2), [this] {
-                        return solo_exit || (!solo_queue.empty() && (exec_half || !exec_on_gpu));
+                        return solo_exit || (!solo_queue.empty() && (exec_shared || !exec_on_gpu));
                     });
                     if (solo_exit) break;
-                    if (solo_queue.empty() || !(exec_half || !exec_on_gpu)) continue;
+                    if (solo_queue.empty() || !(exec_shared || !exec_on_gpu)) continue;
                     sj = solo_queue.front();
                     solo_queue.pop_front();
                     solo_running = true;
@@ -604,7 +649,7 @@ struct Server : ServerBase {
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
                     solo_running = false;
-                    drained = solo_queue.empty() && exec_on_gpu && exec_half;
+                    drained = solo_queue.empty() && exec_on_gpu && exec_shared;
                 }
                 // Nothing left for the solo lane: give the resident exec all its teams back.
                 if (drained) halt_resident();
@@ -623,18 +668,27 @@ struct Server : ServerBase {
                 // Clear a served halt request, then look at the solo lane: submit queues a job
                 // before it requests the halt, so a job queued after this look comes with a
                 // halt that lands after this clear and stops the exec launched below.
-                ck(cudaMemsetAsync(&inst.control.data()->flags, 0, sizeof(unsigned int), exec_s), "clear flags");
+                ck(cudaMemcpyAsync(&inst.control.data()->flags, pinned_ctr + 7, 4, cudaMemcpyHostToDevice, exec_s),
+                   "clear flags");
+                ck(cudaMemcpyAsync(&inst.control.data()->halt_request, pinned_ctr + 7, 4, cudaMemcpyHostToDevice,
+                                   exec_s), "clear halt request");
                 ck(cudaStreamSynchronize(exec_s), "clear flags");
-                bool half;
+                bool shared;
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
-                    half = solo_photons && (!solo_queue.empty() || solo_running);
-                    exec_half = half;
+                    shared = solo_photons && (!solo_queue.empty() || solo_running);
+                    exec_shared = shared;
                     exec_on_gpu = true;
                 }
                 solo_cv.notify_all();
-                P::launch_exec(inst, half ? half_groups : groups, cycles, exec_s);
+                // A shared exec runs a short cycle budget: should the solo job's CTAs not all
+                // find room beside it, the job waits for this exec's end, not for a whole one.
+                const size_t exec_cycles = shared ? std::max<size_t>(cycles / 64u, 4096u) : cycles;
+                trace("exec launched: %s, %zu groups, %zu cycles", shared ? "shared" : "full", shared ? shared_groups : groups,
+                      exec_cycles);
+                P::launch_exec(inst, shared ? shared_groups : groups, exec_cycles, exec_s);
                 cudaError_t le = cudaStreamSynchronize(exec_s);
+                trace("exec ended");
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
                     exec_on_gpu = false;
@@ -680,8 +734,24 @@ struct Server : ServerBase {
             ck(cudaStreamSynchronize(submit_s), "job records");
             done += k;
         }
-        mix_prepare_range_kernel<<<std::min(n, 1184u), 256, 0, submit_s>>>(jobs.data(), first, n);
-        ck(cudaGetLastError(), "output preparation");
+        // Clear the outputs (photon tallies to zero, BFS levels to unreached) with the copy
+        // engine, on the stream that then publishes the jobs.
+        for (unsigned int i = 0; i < n; i++) {
+            const hrm_job& jb = in[i];
+            if (solo_photons && jb.kind == HRM_JOB_PHOTON && jb.count >= solo_photons) continue;  // cleared by its run
+            size_t bytes = 0;
+            const unsigned char* pattern = zeros;
+            if (jb.kind == HRM_JOB_PHOTON) {
+                bytes = ((size_t)jb.n * jb.n * jb.n + 3u * hrm_specs::PHOTON_SPREAD) * sizeof(unsigned long long);
+            } else if (jb.kind == HRM_JOB_BFS) {
+                bytes = (size_t)jb.n * sizeof(unsigned int);
+                pattern = ones;
+            }
+            for (size_t off = 0; off < bytes; off += PATTERN_BYTES) {
+                ck(cudaMemcpyAsync((unsigned char*)jb.out + off, pattern, std::min(PATTERN_BYTES, bytes - off),
+                                   cudaMemcpyHostToDevice, submit_s), "output preparation");
+            }
+        }
         pinned_ctr[0] = first + n;
         // Published after the records (same stream): teams never see a job before its record.
         ck(cudaMemcpyAsync(counters.data(), pinned_ctr, 4, cudaMemcpyHostToDevice, submit_s), "admit");
@@ -692,11 +762,11 @@ struct Server : ServerBase {
             {
                 std::lock_guard<std::mutex> g(solo_lock);
                 for (auto& s : solo) solo_queue.push_back(s);
-                full_on_gpu = exec_on_gpu && !exec_half;
+                full_on_gpu = exec_on_gpu && !exec_shared;
             }
             solo_cv.notify_all();
             // Queued first, then the halt (see loop()): the exec holding every team leaves and
-            // comes back with half of them.
+            // comes back with its share.
             if (full_on_gpu) halt_resident();
         }
         return first;
@@ -889,6 +959,7 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
             size_t used = 0;
             uint32_t admitted = 0, finished = 0;
             std::vector<hrm_job> batch;
+            bool held_back = false;
             auto t0 = clk::now();
             while (finished < njobs) {
                 uint64_t now = ns_since(t0);
@@ -901,7 +972,16 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
                 const size_t free_now = arrivals ? srv->observed_free_bytes() : 0;
                 while (admitted < njobs && arrival_ns[admitted] <= now) {
                     size_t fp = job_footprint(jobs[admitted]);
-                    if ((used + fp > budget || free_now < free_floor) && !inflight.empty()) break;
+                    if ((used + fp > budget || free_now < free_floor) && !inflight.empty()) {
+                        if (!held_back) {
+                            srv->trace("admission held back: %zu B free (floor %zu), %zu B estimated in flight "
+                                       "(budget %zu), %zu jobs in flight", free_now, free_floor, used, budget,
+                                       inflight.size());
+                        }
+                        held_back = true;
+                        break;
+                    }
+                    held_back = false;
                     used += fp;
                     batch.push_back(jobs[admitted]);
                     inflight.push_back(admitted);
@@ -912,6 +992,9 @@ int hrm_serve_replay(const hrm_job* jobs, uint32_t njobs, const uint64_t* arriva
                     uint32_t j = inflight[k];
                     if (done[j] != 0ull) {
                         latency_ns[j] = ns_since(t0) - arrival_ns[j];
+                        if (latency_ns[j] > 100000000ull)
+                            srv->trace("job %u (kind %u, %u items) done after %.1f ms", j, jobs[j].kind,
+                                       (unsigned int)job_sources(jobs[j]), latency_ns[j] / 1e6);
                         used -= job_footprint(jobs[j]);
                         inflight[k] = inflight.back();
                         inflight.pop_back();

@@ -457,21 +457,40 @@ struct hrm_program {
 
 int hrm_capi::set_error(int code, const std::string& msg) { return fail(code, msg); }
 
-unsigned int hrm_capi::photon_teams_per_sm(int variant) {
-    int dev = 0, sms = 1;
+hrm_capi::CtaFootprint hrm_capi::photon_cta_footprint(int variant) {
+    if (variant != HRM_VARIANT_R4_T4_M5) throw std::invalid_argument("photon_cta_footprint: variant not supported");
+    using P = AsyncProgram<MinCtas<hrm_specs::PhotonSpec<4, 4>, 5>>;
+    P::resident_ctas();  // opts the kernel into its dynamic shared memory
+    cudaFuncAttributes fa;
+    ck(cudaFuncGetAttributes(&fa, hrm_rt::async_exec_kernel<P>), "kernel attributes");
+    CtaFootprint f;
+    f.regs_per_thread = (unsigned int)fa.numRegs;
+    f.threads = P::CTA_THREADS;
+    f.smem = fa.sharedSizeBytes + P::SMEM_BYTES;
+    return f;
+}
+
+unsigned int hrm_capi::ctas_beside(const CtaFootprint& a, unsigned int a_ctas, const CtaFootprint& b) {
+    int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0, threads_sm = 0, blocks_sm = 0;
     ck(cudaGetDevice(&dev), "cudaGetDevice");
-    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    unsigned int ctas = 0, teams = 0;
-    switch (variant) {
-        case HRM_VARIANT_R4_T2: {
-            using P = AsyncProgram<hrm_specs::PhotonSpec<4, 2>>;
-            ctas = P::resident_ctas();
-            teams = P::TEAMS_PER_CTA;
-            break;
-        }
-        default: throw std::invalid_argument("photon_teams_per_sm: variant not supported");
+    ck(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev), "attribute");
+    ck(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev), "attribute");
+    ck(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev), "attribute");
+    ck(cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev), "attribute");
+    ck(cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev), "attribute");
+    auto warp_regs = [](unsigned int regs) { return (size_t)((regs * 32u + 255u) / 256u) * 256u; };
+    auto warps = [](const CtaFootprint& f) { return (f.threads + 31u) / 32u; };
+    const size_t part_regs = (size_t)regs_sm / 4u;
+    for (unsigned int c = 64; c > 0; c--) {
+        const size_t smem = (size_t)a_ctas * (a.smem + reserved) + (size_t)c * (b.smem + reserved);
+        const size_t threads = (size_t)a_ctas * a.threads + (size_t)c * b.threads;
+        const size_t regs = (size_t)((a_ctas * warps(a) + 3u) / 4u) * warp_regs(a.regs_per_thread) +
+                            (size_t)((c * warps(b) + 3u) / 4u) * warp_regs(b.regs_per_thread);
+        if (smem <= (size_t)smem_sm && threads <= (size_t)threads_sm && a_ctas + c <= (unsigned int)blocks_sm &&
+            regs <= part_regs)
+            return c;
     }
-    return (ctas / (unsigned int)(sms > 0 ? sms : 1)) * teams;
+    return 0;
 }
 
 #define HRM_GUARD(...)                                           \

@@ -939,10 +939,16 @@ class AsyncProgram {
         const unsigned int my_group = (lane < FN) ? group_of_fn(lane) : NO_GROUP;  // lane f: f's ring group
 
         for (unsigned int cycle = 0; cycle < cycle_count; cycle++) {
-            // Stop on a halt request or an error flag.
+            // Stop on a halt request (halt_early, or the host's halt_request) or an error flag.
             if ((cycle & 31u) == 0) {
                 unsigned int fl = 0;
-                if (lane == 0) fl = hrm_rt::ld_relaxed(&ctl->flags);
+                if (lane == 0) {
+                    fl = hrm_rt::ld_relaxed(&ctl->flags);
+                    if (hrm_rt::ld_relaxed(&ctl->halt_request) != 0u && !(fl & EARLY_HALT_FLAG)) {
+                        atomicOr(&ctl->flags, EARLY_HALT_FLAG);
+                        fl |= EARLY_HALT_FLAG;
+                    }
+                }
                 fl = __shfl_sync(0xFFFFFFFFu, fl, 0);
                 if (fl & (EARLY_HALT_FLAG | hrm_rt::ERROR_MASK)) break;
             }
@@ -1151,6 +1157,7 @@ class AsyncProgram {
             ctx.ctl->flags = 0;
             ctx.ctl->checkout = 0;
             ctx.ctl->done = 0;
+            ctx.ctl->halt_request = 0;
             ctx.ctl->bump = 0;
             ctx.ctl->arena_links = ctx.arena_links;
             ctx.ctl->busy_epoch = 0;

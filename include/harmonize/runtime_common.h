@@ -234,7 +234,10 @@ struct alignas(128) RuntimeControl {
     unsigned int bump;         // arena links handed out lazily so far
     unsigned int arena_links;  // number of links in the arena
     unsigned int generation;   // EventProgram: completed generations
-    unsigned int pad0;
+    // Nonzero: the host asks the running AsyncProgram exec to stop (as halt_early() does). The
+    // host writes it with a copy, so that no kernel launch is needed while a persistent
+    // kernel occupies every SM; the host clears it before the next exec.
+    unsigned int halt_request;
     // [63:40] teams that are busy (not idle, not exited); [39:0] wake-up epoch.
     alignas(128) unsigned long long busy_epoch;
 };
