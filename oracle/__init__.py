@@ -19,4 +19,5 @@ bit for bit with the host executors of the spec sources and with the reference r
 """
 from .lib import (load, max_threads, collatz_range, exec_collatz, bfs, exec_bfs,  # noqa: F401
                   photon_walk, exec_photon, photon_medium, rmat_csr, philox, log, PHOTON_SPREAD,
-                  ref_load, ref_collatz, ref_photon_device, ref_bfs_device, REF_WG, REF_CYCLES)
+                  ref_load, ref_collatz, ref_photon_device, ref_bfs_device, REF_WG, REF_CYCLES,
+                  REF_PHOTON_SHAPE, REF_ASYNC_CLOSED_PHOTON, REF_ASYNC_CLOSED_BFS)

@@ -71,3 +71,16 @@ def test_reference_side_scripts_do_not_load_the_product():
     for rel in ("oracle/reference_bench.py", "oracle/ref_sweep.py", "tests/golden/make_golden.py"):
         src = open(os.path.join(bench.ROOT, rel)).read()
         assert "harmonize_b200" not in src, rel
+
+
+def test_reference_arm_names_resolve():
+    """Every oracle name the reference arm of bench.py uses is exported by the oracle package
+    (the arm only runs on a GPU box; a missing export would end it there)."""
+    import re
+    import oracle
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = open(os.path.join(root, "oracle", "reference_bench.py")).read()
+    names = set(re.findall(r"\boracle\.([A-Za-z_][A-Za-z0-9_]*)", src))
+    assert names, "no oracle names found"
+    missing = [n for n in sorted(names) if not hasattr(oracle, n)]
+    assert not missing, missing
