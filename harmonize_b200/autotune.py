@@ -26,7 +26,7 @@ from . import HERE, VARIANTS, bfs, collatz, photon_medium, photon_walk, rmat_csr
 TUNED_PATH = os.path.join(HERE, "tuned.json")
 PATIENCE = (8, 16, 64)
 FILL_LINKS = (2, 4)
-BATCH_VARIANTS = (0, 1, 2)  # the variants the job-multiplexing spec is built for
+BATCH_VARIANTS = (0, 1, 2, 7, 8)  # the variants the job-multiplexing spec is built for
 
 
 def load_tuned():

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -14,6 +15,13 @@ class AsyncProgram;
 namespace hrm_capi {
 // Records `msg` as the calling thread's last error (read by hrm_last_error) and returns code.
 int set_error(int code, const std::string& msg);
+
+// Tuning adapter: spec BASE compiled for at least MIN_CTAS resident CTAs per SM
+// (__launch_bounds__), which caps its registers.
+template <class BASE, size_t MIN_CTAS>
+struct MinCtas : BASE {
+    static const size_t MIN_CTAS_PER_SM = MIN_CTAS;
+};
 
 // What one CTA of a persistent exec kernel holds on an SM: registers per thread, threads and
 // shared memory (static + dynamic) per CTA.

@@ -263,6 +263,8 @@ struct Batch : BatchBase {
 
 template <size_t R, size_t T>
 using MixAsync = AsyncProgram<hrm_specs::MixSpec<R, T>>;
+template <size_t R, size_t T, size_t M>
+using MixAsyncMin = AsyncProgram<hrm_capi::MinCtas<hrm_specs::MixSpec<R, T>, M>>;
 
 struct BatchKey {
     int dev, variant;
@@ -292,7 +294,9 @@ BatchBase* batch_for(int variant, unsigned int njobs, size_t arena) {
         case HRM_VARIANT_R2_T4: b = new Batch<MixAsync<2, 4>>(cap, arena); break;
         case HRM_VARIANT_R4_T4: b = new Batch<MixAsync<4, 4>>(cap, arena); break;
         case HRM_VARIANT_R4_T2: b = new Batch<MixAsync<4, 2>>(cap, arena); break;
-        default: throw std::invalid_argument("batched runs support variants R2/T4, R4/T4 and R4/T2");
+        case HRM_VARIANT_R4_T2_M11: b = new Batch<MixAsyncMin<4, 2, 11>>(cap, arena); break;
+        case HRM_VARIANT_R4_T4_M5: b = new Batch<MixAsyncMin<4, 4, 5>>(cap, arena); break;
+        default: throw std::invalid_argument("batched runs support variants R2/T4, R4/T4, R4/T2, R4/T2 M11 and R4/T4 M5");
     }
     g_batches.emplace(key, std::unique_ptr<BatchBase>(b));
     return b;
@@ -853,7 +857,9 @@ ServerBase* make_server(unsigned int cap, const hrm_run_config& cfg) {
         case HRM_VARIANT_R2_T4: return new Server<MixAsync<2, 4>>(cap, cfg);
         case HRM_VARIANT_R4_T4: return new Server<MixAsync<4, 4>>(cap, cfg);
         case HRM_VARIANT_R4_T2: return new Server<MixAsync<4, 2>>(cap, cfg);
-        default: throw std::invalid_argument("serving supports variants R2/T4, R4/T4 and R4/T2");
+        case HRM_VARIANT_R4_T2_M11: return new Server<MixAsyncMin<4, 2, 11>>(cap, cfg);
+        case HRM_VARIANT_R4_T4_M5: return new Server<MixAsyncMin<4, 4, 5>>(cap, cfg);
+        default: throw std::invalid_argument("serving supports variants R2/T4, R4/T4, R4/T2, R4/T2 M11 and R4/T4 M5");
     }
 }
 

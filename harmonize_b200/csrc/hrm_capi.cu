@@ -112,12 +112,7 @@ struct LeanRings : BASE {
     };
 };
 
-// Tuning adapter: the spec compiled for at least MIN_CTAS resident CTAs per SM
-// (__launch_bounds__), which caps its registers.
-template <class BASE, size_t MIN_CTAS>
-struct MinCtas : BASE {
-    static const size_t MIN_CTAS_PER_SM = MIN_CTAS;
-};
+using hrm_capi::MinCtas;
 
 // Instantiates spec SPEC<RING, TEAMS> for the chosen program type and tuning variant.
 template <template <size_t, size_t> class SPEC, typename STATE>

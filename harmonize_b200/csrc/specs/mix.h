@@ -333,8 +333,8 @@ HRM_DEV HRM_FI int job_make_work(PROGRAM prog, const MixState& st, unsigned int 
 // another kind's functions, so a team holds promises of one kind at a time and the three
 // kinds' rings share one stash, as large as the photon rings alone. RING: ring links of the
 // photon functions (a move carries a whole photon, 12 words with the job id, a collide 9;
-// every collide batch feeds a batch of tallies, so each needs room for several batches); the
-// Collatz and BFS functions, with 5 words or fewer, get 2*RING links in the same space.
+// every collide batch feeds a batch of tallies, so each needs room for several batches;
+// collides get half); the Collatz and BFS functions, with 5 words or fewer, get 2*RING links.
 template <size_t RING = 4, size_t TEAMS = 4>
 struct MixSpec {
     typedef OpUnion<Job<CollatzEven>, Job<CollatzOdd>, Job<PhotonMove>, Job<PhotonCollide>, Job<PhotonTally>,
@@ -353,9 +353,14 @@ struct MixSpec {
             : (std::is_same<Op, Job<BfsRelax>>::value || std::is_same<Op, Job<BfsExpand>>::value)  ? JOB_BFS
                                                                                                       : JOB_PHOTON;
     };
+    // Photon collides get half the photon ring (at least 2 links): a batch of moves makes at
+    // most one collide per lane.
     template <typename Op>
     struct RING_LINKS_OF {
-        static const size_t value = RING_GROUP_OF<Op>::value == JOB_PHOTON ? RING : 2 * RING;
+        static const size_t value =
+            std::is_same<Op, Job<PhotonCollide>>::value ? (RING / 2 < 2 ? 2 : RING / 2)
+            : RING_GROUP_OF<Op>::value == JOB_PHOTON    ? RING
+                                                        : 2 * RING;
     };
     // BFS jobs take their teams' oldest calls first, as the BFS spec does on its own.
     template <typename Op>

@@ -36,6 +36,7 @@ static_assert(fn_RING_GROUP<Mix42, Job<CollatzEven>>::value == JOB_COLLATZ, "Col
 static_assert(fn_RING_GROUP<Mix42, Job<PhotonCollide>>::value == JOB_PHOTON, "photon group");
 static_assert(fn_RING_GROUP<Mix42, Job<BfsExpand>>::value == JOB_BFS, "BFS group");
 static_assert(fn_RING_LINKS<Mix42, Job<PhotonMove>>::value == 4, "photon rings");
+static_assert(fn_RING_LINKS<Mix42, Job<PhotonCollide>>::value == 2, "photon collide rings: half");
 static_assert(fn_RING_LINKS<Mix42, Job<CollatzEven>>::value == 8, "Collatz rings");
 static_assert(fn_RING_LINKS<Mix42, Job<BfsRelax>>::value == 8, "BFS rings");
 static_assert(fn_OLDEST_FIRST<Mix42, Job<BfsRelax>>::value && fn_OLDEST_FIRST<Mix42, Job<BfsExpand>>::value,
