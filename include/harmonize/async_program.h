@@ -83,6 +83,8 @@ class AsyncProgram {
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
     static const unsigned int COALESCE_PATIENCE =
         (unsigned int)hrm_rt::spec_COALESCE_PATIENCE<PROGRAM_SPEC>::value;
+    static const unsigned int BURST = (unsigned int)hrm_rt::spec_BURST<PROGRAM_SPEC>::value;
+    static_assert(BURST >= 1, "BURST must be at least 1");
 
     static const unsigned int BAD_FUNC_ID_FLAG = hrm_rt::BAD_FUNC_ID_FLAG;
     static const unsigned int STASH_FAIL_FLAG = hrm_rt::STASH_FAIL_FLAG;
@@ -205,10 +207,8 @@ class AsyncProgram {
         unsigned int held_f[HELD_MAX];  // their functions
         // The team's statistics of this exec, kept here rather than in registers (lane 0
         // updates them) and added to the device counters when the team leaves.
-        // n_batch_full: batches in bits 0-31, full batches in bits 32-63 (an exec runs at most
-        // one batch per cycle, and cycle counts are 32-bit); evaluations are counted per
-        // function in fn_evals.
-        unsigned long long n_batch_full, n_spill, n_fill, n_mw, n_idle;
+        // Evaluations are counted per function in fn_evals.
+        unsigned long long n_batches, n_full, n_spill, n_fill, n_mw, n_idle;
         unsigned long long fn_evals[FN];
         unsigned int words[RING_WORDS];
     };
@@ -907,7 +907,8 @@ class AsyncProgram {
             _grp_ctx.held_n = 0;
             _grp_ctx.loads_pending = 0;
             _grp_ctx.overflowed = 0;
-            _grp_ctx.n_batch_full = 0;
+            _grp_ctx.n_batches = 0;
+            _grp_ctx.n_full = 0;
             _grp_ctx.n_spill = 0;
             _grp_ctx.n_fill = 0;
             _grp_ctx.n_mw = 0;
@@ -1086,12 +1087,22 @@ class AsyncProgram {
                 unsigned int rf = __shfl_sync(0xFFFFFFFFu, my_ring, f);
                 spill_fn<0>(f, (cf - (rf - 32u) + 31u) / 32u);
             }
-            run_fn<0>(bf, k);
-            hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
-            settle_overflow();
-            if (lane == 0) {
-                g.n_batch_full += 1ull + ((unsigned long long)(k == 32u) << 32);
-                g.fn_evals[bf] += k;
+            // Evaluate; then, while the function still holds a full batch and every other ring
+            // keeps a batch's worth of room, up to BURST - 1 more batches of it without a
+            // scheduling step (one evaluation site, so the kernel holds one copy of each eval).
+            for (unsigned int rep = 0;; rep++) {
+                run_fn<0>(bf, k);
+                hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
+                settle_overflow();
+                if (lane == 0) {
+                    g.n_batches += 1ull;
+                    g.n_full += (k == 32u);
+                    g.fn_evals[bf] += k;
+                }
+                if (k < 32u || forced || rep + 1u >= BURST) break;
+                const unsigned int cn = (lane < FN) ? g.count[lane] : 0u;
+                if (__shfl_sync(0xFFFFFFFFu, cn, bf) < 32u) break;
+                if (__any_sync(0xFFFFFFFFu, lane < FN && lane != bf && cn + 32u > my_ring)) break;
             }
         }
 
@@ -1123,8 +1134,8 @@ class AsyncProgram {
             }
             unsigned long long* st = _dev_ctx.stats;
             atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);
-            atomicAdd(&st[hrm_rt::STAT_BATCHES], g.n_batch_full & 0xFFFFFFFFull);
-            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_batch_full >> 32);
+            atomicAdd(&st[hrm_rt::STAT_BATCHES], g.n_batches);
+            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_full);
             atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], g.n_spill);
             atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], g.n_fill);
             atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], g.n_mw);
