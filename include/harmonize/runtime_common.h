@@ -217,6 +217,8 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+// Acquire-release fence at GPU scope (lighter than __threadfence's sequentially consistent one).
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
     unsigned int v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -309,7 +311,9 @@ __device__ __forceinline__ bool ring_push(RingSet rs, RuntimeControl* ctl, unsig
     }
     __syncwarp(mask);
     if (j == 0 && n > 0) {
-        __threadfence();
+        // The slots above before the count that announces them (a consumer that sees the
+        // count still waits for each slot's sequence: this orders progress, not data).
+        fence_acq_rel();
         atomicAdd(&rs.heads[r].avail, n);
     }
     return __all_sync(mask, ok);
