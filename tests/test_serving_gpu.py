@@ -52,8 +52,8 @@ def test_replay_completes_every_job(hrm, mix, mode, job_order):
 
 @pytest.mark.gpu
 def test_replay_with_solo_photon_jobs(hrm, mix):
-    """Large photon jobs served alone (the resident kernel pauses): every job completes and
-    every output equals one plain launch per job."""
+    """Large photon jobs served through the solo lane beside the resident kernel: every job
+    completes and every output equals one plain launch per job."""
     from harmonize_b200 import jobs
     n = len(mix.specs)
     counts = sorted(s["count"] for s in mix.specs if s["kind"] == jobs.JOB_PHOTON)
@@ -75,3 +75,29 @@ def test_server_rejects_empty_jobs(hrm, mix):
     with pytest.raises(hrm.HarmonizeError):
         srv.submit(arr)
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", [1, 2])
+def test_jobs_complete_while_a_full_exec_runs(hrm, mix, variant):
+    """Jobs submitted while the resident exec holds every SM (variant 1 fills each SM's register
+    file) complete during that exec: the session clears outputs and publishes jobs with copies
+    only, never with a kernel launch that would wait for the exec to end. The exec's cycle budget
+    (2^24 scheduling rounds, seconds of polling) is far longer than the bound checked here."""
+    from harmonize_b200 import jobs
+    small = [i for i, s in enumerate(mix.specs) if s["kind"] != jobs.JOB_PHOTON][:6]
+    srv = jobs.Server(len(small), arena=1 << 16, cycles=1 << 24, variant=variant)
+    time.sleep(0.05)  # the first exec is on the GPU
+    for k, i in enumerate(small):
+        t0 = time.perf_counter()
+        srv.submit(mix.job_array(0, [i]))
+        while srv.poll()[1] < k + 1:
+            assert time.perf_counter() - t0 < 1.0, f"job {i} not done within 1 s of its submission"
+            time.sleep(0.0005)
+    srv.close()
+    for i in small:
+        s = mix.specs[i]
+        out = mix.output(0, i)
+        if s["kind"] == jobs.JOB_COLLATZ:
+            import oracle
+            assert np.array_equal(out, oracle.collatz_range(s["first"], s["count"]))
