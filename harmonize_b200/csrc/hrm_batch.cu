@@ -447,7 +447,11 @@ struct Server : ServerBase {
     bool solo_running = false;                                // a solo job is on the GPU
     bool exec_shared = false;                                   // the exec on the GPU holds its share beside the solo lane
     bool exec_on_gpu = false;                                 // a resident exec is launched
+    bool solo_full = false;                                   // a solo job holds the whole GPU
     bool solo_exit = false;                                   // the solo runner should stop
+    unsigned int solo_submitted = 0, solo_done = 0;           // solo jobs queued / stamped so far
+    unsigned long long exec_epoch = 0;                         // resident execs launched so far
+    unsigned long long halted_epoch = ~0ull;                   // the exec the solo runner last halted
     size_t shared_groups = 0, solo_groups = 0;
     cudaStream_t solo_s = nullptr;
     std::thread solo_runner;
@@ -583,6 +587,10 @@ struct Server : ServerBase {
     ~Server() {
         host_open = false;
         stop = true;
+        {
+            std::lock_guard<std::mutex> g(solo_lock);  // wakes a resident loop waiting on a solo job
+        }
+        solo_cv.notify_all();
         if (runner.joinable()) {
             pinned_ctr[2] = 0;
             cudaMemcpyAsync(counters.data() + 2, pinned_ctr + 2, 4, cudaMemcpyHostToDevice, submit_s);
@@ -610,16 +618,17 @@ struct Server : ServerBase {
         ck(cudaStreamSynchronize(submit_s), "halt");
     }
 
-    // One solo job on the solo stream, beside the shared resident exec.
-    void run_solo(unsigned int j, const hrm_job& jb) {
+    // One solo job on the solo stream: beside the shared resident exec (groups = solo_groups)
+    // or alone on the GPU (groups = 0: every team that fits).
+    void run_solo(unsigned int j, const hrm_job& jb, size_t groups_) {
         hrm_run_config c;
         memset(&c, 0, sizeof(c));
         c.program_type = HRM_ASYNC;
         c.variant = SOLO_VARIANT;
         c.stream = solo_s;
-        c.groups = solo_groups;
+        c.groups = groups_;
         hrm_run_result r;
-        trace("solo job %u (%u photons) starts", j, jb.count);
+        trace("solo job %u (%u photons) starts %s", j, jb.count, groups_ ? "beside the resident kernel" : "alone");
         if (hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
                                   jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
             throw std::runtime_error(std::string("solo photon job: ") + hrm_last_error());
@@ -631,36 +640,81 @@ struct Server : ServerBase {
         ((volatile unsigned long long*)done_host)[j] = stamp ? stamp : 1ull;
     }
 
-    // The solo runner: serves the solo queue in submission order, one job at a time, only
-    // while the resident exec holds only its share (or no resident exec is running).
+    // Jobs admitted to the resident kernel and not finished yet (solo_lock held).
+    unsigned int resident_in_flight() {
+        const unsigned int total = submitted.load();
+        unsigned int done = 0;
+        for (unsigned int j = 0; j < total; j++) done += ((volatile unsigned long long*)done_host)[j] != 0ull;
+        const unsigned int resident_done = done - std::min(done, solo_done);
+        const unsigned int resident_jobs = total - std::min(total, solo_submitted);
+        return resident_jobs > resident_done ? resident_jobs - resident_done : 0u;
+    }
+
+    // The solo runner: serves the solo queue in submission order, one job at a time. With no
+    // job in flight in the resident kernel, a solo job takes the whole GPU (the resident exec
+    // is halted and not relaunched until the job ends; jobs submitted meanwhile wait in the
+    // table); otherwise it runs beside the resident exec once that holds only its share.
     void solo_loop() {
         try {
             while (true) {
                 std::pair<unsigned int, hrm_job> sj;
+                bool alone = false, halt = false;
                 {
                     std::unique_lock<std::mutex> g(solo_lock);
-                    solo_cv.wait_for(g, std::chrono::milliseconds(2), [this] {
-                        return solo_exit || (!solo_queue.empty() && (exec_shared || !exec_on_gpu));
-                    });
+                    solo_cv.wait_for(g, std::chrono::milliseconds(2),
+                                     [this] { return solo_exit || !solo_queue.empty(); });
                     if (solo_exit) break;
-                    if (solo_queue.empty() || !(exec_shared || !exec_on_gpu)) continue;
+                    if (solo_queue.empty()) continue;
+                    alone = resident_in_flight() == 0u;
+                    if (!alone && exec_on_gpu && !exec_shared) {
+                        // An exec holding every team: ask it once to come back with its share.
+                        halt = halted_epoch != exec_epoch;
+                        halted_epoch = exec_epoch;
+                    }
+                }
+                if (halt) halt_resident();
+                {
+                    std::unique_lock<std::mutex> g(solo_lock);
+                    if (solo_queue.empty()) continue;
+                    alone = resident_in_flight() == 0u;
+                    if (!alone && !(exec_shared || !exec_on_gpu)) continue;  // wait for the shared exec
                     sj = solo_queue.front();
                     solo_queue.pop_front();
                     solo_running = true;
+                    solo_full = alone;
                 }
-                run_solo(sj.first, sj.second);
+                if (alone) {
+                    bool running;
+                    {
+                        std::lock_guard<std::mutex> g(solo_lock);
+                        running = exec_on_gpu;
+                    }
+                    if (running) halt_resident();
+                    std::unique_lock<std::mutex> g(solo_lock);
+                    solo_cv.wait(g, [this] { return !exec_on_gpu || solo_exit; });
+                    if (solo_exit) break;
+                }
+                run_solo(sj.first, sj.second, alone ? 0u : solo_groups);
                 bool drained;
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
                     solo_running = false;
+                    solo_full = false;
+                    solo_done++;
                     drained = solo_queue.empty() && exec_on_gpu && exec_shared;
                 }
+                solo_cv.notify_all();
                 // Nothing left for the solo lane: give the resident exec all its teams back.
                 if (drained) halt_resident();
             }
         } catch (std::exception& e) {
-            std::lock_guard<std::mutex> g(err_lock);
-            err = e.what();
+            {
+                std::lock_guard<std::mutex> g(err_lock);
+                err = e.what();
+            }
+            std::lock_guard<std::mutex> g(solo_lock);
+            solo_full = false;  // never leave the resident loop waiting
+            solo_cv.notify_all();
         }
     }
 
@@ -679,10 +733,14 @@ struct Server : ServerBase {
                 ck(cudaStreamSynchronize(exec_s), "clear flags");
                 bool shared;
                 {
-                    std::lock_guard<std::mutex> g(solo_lock);
+                    // A solo job that holds the whole GPU keeps the resident kernel off it.
+                    std::unique_lock<std::mutex> g(solo_lock);
+                    solo_cv.wait(g, [this] { return !solo_full || stop; });
+                    if (stop) break;
                     shared = solo_photons && (!solo_queue.empty() || solo_running);
                     exec_shared = shared;
                     exec_on_gpu = true;
+                    exec_epoch++;
                 }
                 solo_cv.notify_all();
                 // A shared exec runs a short cycle budget: should the solo job's CTAs not all
@@ -697,6 +755,7 @@ struct Server : ServerBase {
                     std::lock_guard<std::mutex> g(solo_lock);
                     exec_on_gpu = false;
                 }
+                solo_cv.notify_all();
                 ck(le, "serving exec");
                 unsigned int f = inst.flags();
                 if (f & hrm_rt::ERROR_MASK) hrm_rt::throw_flags(f);
@@ -709,8 +768,13 @@ struct Server : ServerBase {
                 if (!host_open && (f & hrm_rt::COMPLETION_FLAG) && !solo_left) break;
             }
         } catch (std::exception& e) {
-            std::lock_guard<std::mutex> g(err_lock);
-            err = e.what();
+            {
+                std::lock_guard<std::mutex> g(err_lock);
+                err = e.what();
+            }
+            std::lock_guard<std::mutex> g(solo_lock);
+            exec_on_gpu = false;  // never leave the solo runner waiting for this loop
+            solo_cv.notify_all();
         }
     }
 
@@ -766,11 +830,14 @@ struct Server : ServerBase {
             {
                 std::lock_guard<std::mutex> g(solo_lock);
                 for (auto& s : solo) solo_queue.push_back(s);
-                full_on_gpu = exec_on_gpu && !exec_shared;
+                solo_submitted += (unsigned int)solo.size();
+                // With jobs in flight the solo lane will share the GPU: the exec holding every
+                // team must come back with its share. (With none, the solo runner halts it and
+                // takes the whole GPU.)
+                full_on_gpu = exec_on_gpu && !exec_shared && resident_in_flight() > 0u;
             }
             solo_cv.notify_all();
-            // Queued first, then the halt (see loop()): the exec holding every team leaves and
-            // comes back with its share.
+            // Queued first, then the halt (see loop()).
             if (full_on_gpu) halt_resident();
         }
         return first;
