@@ -63,8 +63,9 @@ def parse():
                    help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
     p.add_argument("--solo-photons", type=int, default=1 << 15,
                    help="batched: photon jobs at least this large also run alone (the persistent_solo arm)")
-    p.add_argument("--serve-solo-photons", type=int, default=1 << 17,
-                   help="serving: photon jobs at least this large run alone (0 = never)")
+    p.add_argument("--serve-solo-photons", type=int, default=1 << 13,
+                   help="serving: photon jobs at least this large run through the solo lane (0 = never); "
+                        "2^13 from a sweep of 2^13..2^17 (lowest p50 at every load and p99 at 1.0+)")
     return p.parse_args()
 
 
@@ -481,7 +482,7 @@ def run_serving(args):
     mism = [i for i in range(n) if not (np.array_equal(mix.output(0, i), mix.output(1, i)) and
                                         np.array_equal(mix.output(0, i), mix.output(2, i)))]
     line = {"metric": "job latency p50/p99/p99.9 (ms) and job throughput", "workload": f"serving_{n}_jobs",
-            "saturation_jobs_per_s": round(sat, 1), "rates": rows,
+            "saturation_jobs_per_s": round(sat, 1), "solo_photons": args.serve_solo_photons, "rates": rows,
             "outputs": "identical per job" if not mism else f"{len(mism)} jobs differ"}
     print(json.dumps(line), flush=True)
     return line
