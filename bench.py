@@ -63,6 +63,9 @@ def parse():
                    help="batched/serving: which job make_work serves (HRM_JOB_ORDER_*)")
     p.add_argument("--solo-photons", type=int, default=1 << 15,
                    help="batched: photon jobs at least this large also run alone (the persistent_solo arm)")
+    p.add_argument("--solo-lanes", type=int, default=3,
+                   help="batched: concurrent lanes of the persistent_solo arm's large jobs (1..8; 3 from a sweep "
+                        "of 1..4 on the 4096-job mix)")
     p.add_argument("--serve-solo-photons", type=int, default=1 << 13,
                    help="serving: photon jobs at least this large run through the solo lane (0 = never); "
                         "2^13 from a sweep of 2^13..2^17 (lowest p50 at every load and p99 at 1.0+)")
@@ -408,6 +411,10 @@ def run_batched(args):
     jobs.batch_run(mix, 0, warm, **tc)
     jobs.plain_run(mix, 1, warm)
     jobs.runtime_run(mix, 2, warm)
+    # The solo lanes' program instances are made on first use: warm them up on a few large jobs.
+    solo_warm = [i for i, s in enumerate(specs)
+                 if s["kind"] == jobs.JOB_PHOTON and s["count"] >= args.solo_photons][:max(1, args.solo_lanes)]
+    jobs.batch_run_solo(mix, 3, indices=solo_warm, solo_photons=args.solo_photons, lanes=args.solo_lanes, **tc)
     with ClockSampler(0) as clk:
         done_b, res = jobs.batch_run(mix, 0, **tc)
         torch.cuda.synchronize()
@@ -415,7 +422,7 @@ def run_batched(args):
         torch.cuda.synchronize()
         done_r, runtime_ms = jobs.runtime_run(mix, 2)
         torch.cuda.synchronize()
-        done_s, solo_ms, _ = jobs.batch_run_solo(mix, 3, solo_photons=args.solo_photons, **tc)
+        done_s, solo_ms, _ = jobs.batch_run_solo(mix, 3, solo_photons=args.solo_photons, lanes=args.solo_lanes, **tc)
     for other, name in ((1, "plain-kernel"), (2, "per-job runtime"), (3, "persistent with solo large jobs")):
         mism = [i for i in range(len(specs)) if not np.array_equal(mix.output(0, i), mix.output(other, i))]
         if mism:
@@ -432,8 +439,9 @@ def run_batched(args):
                    "runtime_per_job": "one whole single-spec AsyncProgram run per job (init, exec until "
                                       "complete, synchronised), tuned variant per kind",
                    "plain": "one hand-written plain kernel launch per job (one thread per item), 16 streams",
-                   "persistent_solo": f"photon jobs of >= {args.solo_photons} photons one by one through the "
-                                      "single-spec runtime, all other jobs in one persistent launch"},
+                   "persistent_solo": f"photon jobs of >= {args.solo_photons} photons through the single-spec "
+                                      f"runtime over {args.solo_lanes} concurrent lanes (hrm_solo_run), all other "
+                                      "jobs in one persistent launch"},
         "jobs_per_s": {"persistent": round(args.jobs / (span_b / 1e3), 1),
                        "persistent_solo": round(args.jobs / (solo_ms / 1e3), 1),
                        "runtime_per_job": round(args.jobs / (runtime_ms / 1e3), 1),

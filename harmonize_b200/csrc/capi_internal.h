@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/hrm_capi.h"
+
 #include <cstddef>
 #include <stdexcept>
 #include <string>
@@ -30,6 +32,16 @@ struct CtaFootprint {
     unsigned int threads = 0;
     size_t smem = 0;
 };
+
+// A photon walk through the whole-run helper (hrm_photon_run_device) on the cached program
+// instance of `lane`: walks on different lanes may run at once (on different streams).
+int photon_walk_lane(unsigned int lane, const float* d_mu_s, const float* d_absorb, const uint8_t* d_split,
+                     uint32_t n, uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally,
+                     const hrm_run_config* cfg, hrm_run_result* res);
+
+// Teams of the single-spec photon-walk AsyncProgram of tuning variant `variant` that fit on
+// the current device at once.
+size_t photon_resident_teams(int variant);
 
 // The CTA footprint of the single-spec photon-walk AsyncProgram exec kernel of tuning variant
 // `variant` on the current device (HRM_VARIANT_R4_T4_M5 only).

@@ -1263,6 +1263,84 @@ int hrm_runtime_run(const hrm_job* jobs, uint32_t njobs, int program_type, const
     }
 }
 
+int hrm_solo_run(const hrm_job* jobs, uint32_t njobs, int variant, uint32_t nlanes, uint64_t* done_ns,
+                 float* total_ms) {
+    if (jobs == nullptr && njobs != 0) return hrm_capi::set_error(HRM_EINVAL, "jobs is NULL");
+    if (nlanes == 0 || nlanes > 8) return hrm_capi::set_error(HRM_EINVAL, "nlanes must be 1..8");
+    try {
+        for (uint32_t j = 0; j < njobs; j++) {
+            validate(jobs[j]);
+            if (jobs[j].kind != HRM_JOB_PHOTON) throw std::invalid_argument("hrm_solo_run takes photon jobs only");
+        }
+        int dev = 0;
+        ck(cudaGetDevice(&dev), "cudaGetDevice");
+        const size_t teams = hrm_capi::photon_resident_teams(variant);
+        const size_t lane_groups = std::max<size_t>(2, (teams / nlanes) & ~(size_t)1);
+        std::vector<cudaStream_t> streams(nlanes, nullptr);
+        auto release = hrm_capi::on_scope_exit([&] {
+            for (auto& st : streams)
+                if (st) cudaStreamDestroy(st);
+        });
+        for (auto& st : streams) ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        ck(cudaDeviceSynchronize(), "sync");
+        std::atomic<uint32_t> next{0};
+        std::atomic<bool> failed{false};
+        std::mutex err_lock;
+        int err_code = HRM_OK;
+        std::string err_msg;
+        const auto t0 = std::chrono::steady_clock::now();
+        auto lane_main = [&](unsigned int lane) {
+            if (cudaSetDevice(dev) != cudaSuccess) {
+                failed = true;
+                return;
+            }
+            hrm_run_config cfg;
+            memset(&cfg, 0, sizeof(cfg));
+            cfg.program_type = HRM_ASYNC;
+            cfg.variant = variant;
+            cfg.stream = streams[lane];
+            cfg.groups = nlanes > 1 ? lane_groups : 0;
+            while (!failed) {
+                const uint32_t j = next++;
+                if (j >= njobs) break;
+                const hrm_job& jb = jobs[j];
+                hrm_run_result res;
+                const int rc = hrm_capi::photon_walk_lane(lane, (const float*)jb.a, (const float*)jb.b,
+                                                          (const uint8_t*)jb.c, jb.n, jb.seed, jb.first, jb.count,
+                                                          (uint64_t*)jb.out, &cfg, &res);
+                if (rc != HRM_OK) {
+                    std::lock_guard<std::mutex> g(err_lock);
+                    if (err_code == HRM_OK) {
+                        err_code = rc;
+                        err_msg = hrm_last_error();
+                    }
+                    failed = true;
+                    break;
+                }
+                if (done_ns) {
+                    done_ns[j] = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                     std::chrono::steady_clock::now() - t0)
+                                     .count();
+                }
+            }
+        };
+        std::vector<std::thread> threads;
+        for (unsigned int lane = 1; lane < nlanes; lane++) threads.emplace_back(lane_main, lane);
+        lane_main(0);
+        for (auto& t : threads) t.join();
+        if (total_ms) {
+            *total_ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (err_code != HRM_OK) return hrm_capi::set_error(err_code, err_msg);
+        if (failed) return hrm_capi::set_error(HRM_ECUDA, "cudaSetDevice failed on a lane thread");
+        return HRM_OK;
+    } catch (std::invalid_argument& e) {
+        return hrm_capi::set_error(HRM_EINVAL, e.what());
+    } catch (std::exception& e) {
+        return hrm_capi::set_error(HRM_ECUDA, e.what());
+    }
+}
+
 int hrm_plain_run(const hrm_job* jobs, uint32_t njobs, uint32_t nstreams, uint64_t* done_ns, float* total_ms) {
     if (jobs == nullptr && njobs != 0) return hrm_capi::set_error(HRM_EINVAL, "jobs is NULL");
     if (nstreams == 0) nstreams = 1;

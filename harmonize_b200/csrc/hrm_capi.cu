@@ -51,6 +51,8 @@ struct ProgramBase {
     virtual std::vector<unsigned int> overview() = 0;
     virtual void set_state(const void* state, size_t size) = 0;
     virtual void set_tuning(unsigned int patience, unsigned int fill_links) = 0;
+    // Teams of an AsyncProgram exec that fit on the device at once (0 for EventProgram).
+    virtual size_t resident_teams() = 0;
     // Device scratch of the whole-run helpers (the start-value / source iterator), kept with
     // the instance so that cached runs allocate nothing.
     util::host::DevBuf<util::iter::AtomicIter<unsigned int>> iterator{(size_t)1};
@@ -77,6 +79,13 @@ struct ProgramImpl : ProgramBase {
     void set_state(const void* state, size_t size) override {
         if (size != sizeof(typename P::DeviceState)) throw std::invalid_argument("device state size mismatch");
         memcpy((void*)&inst.device_state, state, size);
+    }
+    size_t resident_teams() override {
+        if constexpr (hrm_capi::is_async_program<P>::value) {
+            return (size_t)P::resident_ctas() * P::TEAMS_PER_CTA;
+        } else {
+            return 0;
+        }
     }
     void set_tuning(unsigned int patience, unsigned int fill_links) override {
         if constexpr (hrm_capi::is_async_program<P>::value) {
@@ -292,8 +301,10 @@ std::shared_ptr<Staging> staging() {
 struct CacheKey {
     int dev, spec, type, variant;
     size_t arena;
+    unsigned int lane;  // concurrent runs of one configuration use instances of different lanes
     bool operator<(const CacheKey& o) const {
-        return std::tie(dev, spec, type, variant, arena) < std::tie(o.dev, o.spec, o.type, o.variant, o.arena);
+        return std::tie(dev, spec, type, variant, arena, lane) <
+               std::tie(o.dev, o.spec, o.type, o.variant, o.arena, o.lane);
     }
 };
 std::mutex g_cache_mutex;
@@ -302,10 +313,11 @@ std::map<CacheKey, std::shared_ptr<ProgramBase>> g_cache;
 // Shared ownership, as for staging: a run holds its instance until it ends, even if
 // hrm_release_cache drops the cache's reference meanwhile.
 template <typename STATE>
-std::shared_ptr<ProgramBase> cached_program(int spec, int type, int variant, size_t arena, const STATE& st) {
+std::shared_ptr<ProgramBase> cached_program(int spec, int type, int variant, size_t arena, const STATE& st,
+                                            unsigned int lane = 0) {
     int dev = 0;
     ck(cudaGetDevice(&dev), "cudaGetDevice");
-    CacheKey key{dev, spec, type, variant, arena};
+    CacheKey key{dev, spec, type, variant, arena, lane};
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     auto it = g_cache.find(key);
     if (it == g_cache.end()) {
@@ -342,9 +354,11 @@ int collatz_run(uint32_t start, uint32_t count, uint32_t* d_out, const hrm_run_c
     return run_to_completion(p.get(), cfg, res);
 }
 
-// Photon walk with device-resident medium and tally (tally zeroed here).
-int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32_t n, uint64_t seed, uint32_t first,
-               uint32_t count, uint64_t* d_tally, const hrm_run_config* cfg_in, hrm_run_result* res) {
+// Photon walk with device-resident medium and tally (tally zeroed here), on the cached
+// instance of `lane` (concurrent walks of one configuration use different lanes).
+int photon_run_lane(unsigned int lane, const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32_t n,
+                    uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally, const hrm_run_config* cfg_in,
+                    hrm_run_result* res) {
     hrm_run_config cfg = config_or_default(cfg_in);
     if (n < 2 || n > 1024 || (n & 1u)) return fail(HRM_EINVAL, "grid edge must be even and in [2, 1024]");
     if ((uint64_t)first + count > 0xFFFFFFFFull) return fail(HRM_EINVAL, "first + count exceeds 2^32");
@@ -365,13 +379,18 @@ int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32
     // splits grow a batch of photons several-fold before roulette thins it.
     st.load_limit = 0.015625f;
     size_t arena = cfg.arena ? cfg.arena : default_arena(HRM_SPEC_PHOTON, cfg.program_type);
-    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_PHOTON, cfg.program_type, cfg.variant, arena, st);
+    std::shared_ptr<ProgramBase> p = cached_program(HRM_SPEC_PHOTON, cfg.program_type, cfg.variant, arena, st, lane);
     std::lock_guard<std::mutex> run(p->run_lock);
     util::iter::AtomicIter<unsigned int> host_it(first, first + count);
     ck(cudaMemcpyAsync(p->iterator.data(), &host_it, sizeof(host_it), cudaMemcpyHostToDevice, s), "iterator upload");
     st.source = p->iterator.data();
     p->set_state(&st, sizeof(st));
     return run_to_completion(p.get(), cfg, res);
+}
+
+int photon_run(const float* d_mu, const float* d_ab, const uint8_t* d_sp, uint32_t n, uint64_t seed, uint32_t first,
+               uint32_t count, uint64_t* d_tally, const hrm_run_config* cfg_in, hrm_run_result* res) {
+    return photon_run_lane(0, d_mu, d_ab, d_sp, n, seed, first, count, d_tally, cfg_in, res);
 }
 
 // BFS over a device-resident CSR graph; levels initialised here.
@@ -503,6 +522,21 @@ unsigned int hrm_capi::ctas_beside(const CtaFootprint& a, unsigned int a_ctas, c
 
 // Forgets the kept device addresses of the no-allocation scratch area (defined below).
 void noalloc_forget_addresses();
+
+int hrm_capi::photon_walk_lane(unsigned int lane, const float* d_mu_s, const float* d_absorb, const uint8_t* d_split,
+                               uint32_t n, uint64_t seed, uint32_t first, uint32_t count, uint64_t* d_tally,
+                               const hrm_run_config* cfg, hrm_run_result* res) {
+    if (!d_mu_s || !d_absorb || !d_split || !d_tally) return fail(HRM_EINVAL, "NULL buffer");
+    HRM_GUARD(return photon_run_lane(lane, d_mu_s, d_absorb, d_split, n, seed, first, count, d_tally, cfg, res);)
+}
+
+size_t hrm_capi::photon_resident_teams(int variant) {
+    hrm_specs::PhotonState st;
+    memset(&st, 0, sizeof(st));
+    std::shared_ptr<ProgramBase> p =
+        cached_program(HRM_SPEC_PHOTON, HRM_ASYNC, variant, default_arena(HRM_SPEC_PHOTON, HRM_ASYNC), st);
+    return p->resident_teams();
+}
 
 extern "C" {
 

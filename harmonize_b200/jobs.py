@@ -50,6 +50,7 @@ def _bind():
             "hrm_server_close": [vp, u32],
             "hrm_server_destroy": [vp],
             "hrm_serve_replay": [vp, u32, vp, ctypes.c_int, u32, vp, vp, ctypes.POINTER(ctypes.c_float)],
+            "hrm_solo_run": [vp, u32, ctypes.c_int, u32, vp, ctypes.POINTER(ctypes.c_float)],
         }.items():
             f = getattr(L, name)
             f.restype = ctypes.c_int
@@ -208,13 +209,15 @@ def batch_run(mix, which=0, indices=None, **cfg_kw):
     return done, res.as_dict()
 
 
-def batch_run_solo(mix, which=0, solo_photons=1 << 15, indices=None, **cfg_kw):
+def batch_run_solo(mix, which=0, solo_photons=1 << 15, indices=None, lanes=1, **cfg_kw):
     """The batch with its largest jobs taken out of the persistent launch.
 
     Photon jobs of at least `solo_photons` photons each fill the GPU on their own, so running
     them among the other jobs gains them nothing and costs them the job indirection of the
-    multiplexing kernel (about half its speed on photon work). They run one after another
-    through the single-spec runtime, after one persistent launch of all the other jobs.
+    multiplexing kernel (about half its speed on photon work). They run through the
+    single-spec runtime after one persistent launch of all the other jobs: one after another
+    (lanes=1), or over `lanes` concurrent lanes that share the GPU (hrm_solo_run), so that each
+    job's tail of dependent calls overlaps the others' work.
     Returns (done_ns per job from the start of the batch, total ms, result of the persistent
     launch or None)."""
     idx = list(range(len(mix.specs))) if indices is None else list(indices)
@@ -229,7 +232,18 @@ def batch_run_solo(mix, which=0, solo_photons=1 << 15, indices=None, **cfg_kw):
         for k, i in enumerate(rest):
             done[pos[i]] = d[k]
         total_ms += res["device_ms"]
-    if solo:
+    if solo and lanes > 1:
+        from .autotune import tuned_variant
+        L = _bind()
+        arr = mix.job_array(which, solo)
+        d = np.zeros(len(arr), dtype=np.uint64)
+        total = ctypes.c_float()
+        check(L.hrm_solo_run(ctypes.byref(arr), len(arr), tuned_variant("photon", "async"), lanes, d.ctypes.data,
+                             ctypes.byref(total)))
+        for k, i in enumerate(solo):
+            done[pos[i]] = d[k] + np.uint64(total_ms * 1e6)
+        total_ms += total.value
+    elif solo:
         d, ms = runtime_run(mix, which, indices=solo)
         for k, i in enumerate(solo):
             done[pos[i]] = d[k] + np.uint64(total_ms * 1e6)

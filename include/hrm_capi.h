@@ -275,6 +275,14 @@ int hrm_plain_run(const hrm_job* jobs, uint32_t njobs, uint32_t nstreams, uint64
  * (host clock, ns from the first job's start) and *total_ms as above. */
 int hrm_runtime_run(const hrm_job* jobs, uint32_t njobs, int program_type, const int* variants, uint64_t* done_ns,
                     float* total_ms);
+/* Large photon jobs through the single-spec AsyncProgram (no counterpart in the original): the
+ * jobs (all HRM_JOB_PHOTON) run in order over nlanes lanes (1..8), each lane a host thread
+ * with its own stream and program instance and 1/nlanes of the teams that fit on the device,
+ * so that one job's tail of dependent calls overlaps the others' work. variant: the compiled
+ * photon variant. done_ns (host clock, ns from the start of the call) and *total_ms as above.
+ * Outputs equal one run per job, bit for bit. */
+int hrm_solo_run(const hrm_job* jobs, uint32_t njobs, int variant, uint32_t nlanes, uint64_t* done_ns,
+                 float* total_ms);
 
 /* ---- serving: a resident runtime admitting jobs while it runs ---------------------------
  * No counterpart in the original. hrm_server_open starts a persistent AsyncProgram over the

@@ -51,13 +51,15 @@ def test_batch_subset_and_repeat(hrm, small_mix):
 
 
 @pytest.mark.gpu
-def test_batch_with_solo_large_jobs_equals_plain(hrm, small_mix):
-    """Large photon jobs run alone through the single-spec runtime, the rest in one launch:
-    every output still equals one plain launch per job."""
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_batch_with_solo_large_jobs_equals_plain(hrm, small_mix, lanes):
+    """Large photon jobs run through the single-spec runtime (one after another, or over three
+    concurrent lanes that share the GPU), the rest in one launch: every output still equals one
+    plain launch per job."""
     from harmonize_b200 import jobs
     counts = sorted(s["count"] for s in small_mix.specs if s["kind"] == jobs.JOB_PHOTON)
     threshold = counts[len(counts) // 2]  # about half of the photon jobs run alone
-    done, total_ms, res = jobs.batch_run_solo(small_mix, which=0, solo_photons=threshold, job_order=1)
+    done, total_ms, res = jobs.batch_run_solo(small_mix, which=0, solo_photons=threshold, job_order=1, lanes=lanes)
     assert total_ms > 0 and res is not None and (done > 0).all()
     jobs.plain_run(small_mix, which=1, streams=4)
     for i, s in enumerate(small_mix.specs):

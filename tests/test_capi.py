@@ -84,6 +84,15 @@ def test_job_and_input_entry_points_reject_bad_arguments(hrm):
     assert L.hrm_plain_run(None, u32(3), u32(4), None, None) == hrm.HRM_EINVAL
     assert L.hrm_runtime_run(None, u32(3), 0, None, None, None) == hrm.HRM_EINVAL
     assert L.hrm_serve_replay(None, u32(3), None, 0, u32(1), None, None, None) == hrm.HRM_EINVAL
+    from harmonize_b200 import jobs
+    J = jobs._bind()
+    assert J.hrm_solo_run(None, u32(3), 7, u32(2), None, None) == hrm.HRM_EINVAL       # no jobs
+    one = (jobs.Job * 1)()
+    one[0] = jobs.Job(jobs.JOB_COLLATZ, 1, 16, 0, 0, None, None, None, 0x1000)
+    assert J.hrm_solo_run(ctypes.byref(one), u32(1), 7, u32(0), None, None) == hrm.HRM_EINVAL   # no lane
+    assert J.hrm_solo_run(ctypes.byref(one), u32(1), 7, u32(9), None, None) == hrm.HRM_EINVAL   # too many
+    assert J.hrm_solo_run(ctypes.byref(one), u32(1), 7, u32(2), None, None) == hrm.HRM_EINVAL   # not photon
+    assert "photon jobs only" in hrm.lib().hrm_last_error().decode()
     rp = np.zeros(5, dtype=np.uint32)
     col = np.zeros(16, dtype=np.uint32)
     assert L.hrm_rmat_csr(2, 4, ctypes.c_double(0.6), ctypes.c_double(0.3), ctypes.c_double(0.3), ctypes.c_uint64(1),
