@@ -257,8 +257,8 @@ typedef struct hrm_job {
 
 /* All jobs in ONE persistent AsyncProgram launch (job-multiplexing spec; the launch sequence
  * is a CUDA graph replayed per call). done_ns (host, njobs entries, may be NULL) receives each
- * job's completion time in ns after the start of the device work. cfg->variant: R2/T4, R4/T4
- * or R4/T2. Outputs equal those of one run per job, bit for bit. The batch context (instance,
+ * job's completion time in ns after the start of the device work. cfg->variant: R2/T4, R4/T4,
+ * R4/T2, R4/T2 M11 or R4/T4 M5. Outputs equal those of one run per job, bit for bit. The batch context (instance,
  * job table and graph, per device, variant, job capacity rounded up to a power of two and
  * arena) is kept for the next call until the process exits; calls on one context are
  * serialised. */
