@@ -441,20 +441,26 @@ struct Server : ServerBase {
     unsigned int solo_photons;
     // The solo lane's photon kernel: 4 teams per CTA (one warp per SM sub-partition).
     static const int SOLO_VARIANT = HRM_VARIANT_R4_T4_M5;
+    // Solo jobs run on SOLO_LANES lanes at once (a runner thread, a stream and a program
+    // instance each), every lane with its share of the solo lane's teams, so that one job's
+    // tail of dependent calls overlaps the other's work.
+    static const unsigned int SOLO_LANES = 2;
     std::mutex solo_lock;                                     // guards the fields below
     std::condition_variable solo_cv;
     std::deque<std::pair<unsigned int, hrm_job>> solo_queue;  // (job index, job)
-    bool solo_running = false;                                // a solo job is on the GPU
-    bool exec_shared = false;                                   // the exec on the GPU holds its share beside the solo lane
+    unsigned int solo_active = 0;                             // solo jobs on the GPU
+    bool exec_shared = false;                                 // the exec on the GPU holds its share beside the solo lane
     bool exec_on_gpu = false;                                 // a resident exec is launched
-    bool solo_full = false;                                   // a solo job holds the whole GPU
-    bool solo_exit = false;                                   // the solo runner should stop
+    unsigned int solo_alone = 0;                              // solo jobs that keep the resident kernel off the GPU
+    bool solo_exit = false;                                   // the solo runners should stop
     unsigned int solo_submitted = 0, solo_done = 0;           // solo jobs queued / stamped so far
     unsigned long long exec_epoch = 0;                         // resident execs launched so far
     unsigned long long halted_epoch = ~0ull;                   // the exec the solo runner last halted
-    size_t shared_groups = 0, solo_groups = 0;
-    cudaStream_t solo_s = nullptr;
-    std::thread solo_runner;
+    // Teams of a solo job beside the resident kernel / with it off the GPU: the whole share
+    // for a job that runs by itself, a lane's share while several run.
+    size_t shared_groups = 0, solo_groups = 0, alone_groups = 0, solo_groups_lane = 0, alone_groups_lane = 0;
+    cudaStream_t solo_s[SOLO_LANES] = {};
+    std::vector<std::thread> solo_runners;
     unsigned long long* done_dev = nullptr;                    // device alias of done_host
 
     Server(unsigned int cap, const hrm_run_config& cfg)
@@ -473,7 +479,9 @@ struct Server : ServerBase {
             throw;
         }
         runner = std::thread([this] { loop(); });
-        if (solo_photons) solo_runner = std::thread([this] { solo_loop(); });
+        if (solo_photons) {
+            for (unsigned int lane = 0; lane < SOLO_LANES; lane++) solo_runners.emplace_back([this, lane] { solo_loop(lane); });
+        }
     }
 
     void set_up(unsigned int cap, const hrm_run_config& cfg) {
@@ -518,8 +526,7 @@ struct Server : ServerBase {
             clock_offset_ns = (long long)g - mid;
         }
         if (solo_photons) {
-            // Half of each kernel's resident teams per SM: two halves fit one SM together.
-            ck(cudaStreamCreateWithFlags(&solo_s, cudaStreamNonBlocking), "stream");
+            for (auto& st : solo_s) ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
             int dev = 0, sms = 1;
             ck(cudaGetDevice(&dev), "cudaGetDevice");
             ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
@@ -540,35 +547,49 @@ struct Server : ServerBase {
             while (m > 0 && (s = hrm_capi::ctas_beside(mix_cta, m, solo_cta)) == 0) m--;
             if (m == 0 || s == 0) throw std::runtime_error("solo lane: the photon kernel fits beside no resident CTA");
             shared_groups = (size_t)m * (size_t)sms * P::TEAMS_PER_CTA;
-            solo_groups = (size_t)s * (size_t)sms * (solo_cta.threads / 32u);
+            const size_t cta_teams = solo_cta.threads / 32u;
+            auto per_lane = [&](size_t teams) {  // one lane's share, in whole CTAs, at least one CTA
+                const size_t g = teams / SOLO_LANES / cta_teams * cta_teams;
+                return g > cta_teams ? g : cta_teams;
+            };
+            solo_groups = (size_t)s * (size_t)sms * cta_teams;
+            alone_groups = hrm_capi::photon_resident_teams(SOLO_VARIANT);
+            solo_groups_lane = per_lane(solo_groups);
+            alone_groups_lane = per_lane(alone_groups);
             trace("solo lane: resident %u of %u CTAs per SM (%u regs, %zu B), solo photon %u CTAs per SM "
-                  "(%u regs, %zu B): shared_groups %zu solo_groups %zu",
-                  m, mix_ctas_per_sm, mix_cta.regs_per_thread, mix_cta.smem, s, solo_cta.regs_per_thread,
-                  solo_cta.smem, shared_groups, solo_groups);
+                  "(%u regs, %zu B): shared_groups %zu; solo teams beside it %zu (a lane's share %zu), alone %zu "
+                  "(%zu)", m, mix_ctas_per_sm, mix_cta.regs_per_thread, mix_cta.smem, s, solo_cta.regs_per_thread,
+                  solo_cta.smem, shared_groups, solo_groups, solo_groups_lane, alone_groups, alone_groups_lane);
             // The solo job's kernel must start before the shared exec may be counted on:
             // load it now (lazy loading would hold it back until a running kernel ends).
-            hrm_run_config c;
-            memset(&c, 0, sizeof(c));
-            c.program_type = HRM_ASYNC;
-            c.variant = SOLO_VARIANT;
-            c.stream = solo_s;
-            c.groups = solo_groups;
+            // Every lane's program instance is made now too (it allocates its arena).
             util::host::DevBuf<float> mu((size_t)8);
             util::host::DevBuf<unsigned char> sp((size_t)8);
             util::host::DevBuf<unsigned long long> t((size_t)(8 + 3 * hrm_specs::PHOTON_SPREAD));
             ck(cudaMemset(mu.data(), 0, 8 * sizeof(float)), "warm-up medium");
             ck(cudaMemset(sp.data(), 0, 8), "warm-up medium");
-            hrm_run_result r;
-            if (hrm_photon_run_device(mu.data(), mu.data(), sp.data(), 2, 1, 0, 0, (uint64_t*)t.data(), &c, &r) != HRM_OK)
-                throw std::runtime_error(std::string("solo lane warm-up: ") + hrm_last_error());
+            for (unsigned int lane = 0; lane < SOLO_LANES; lane++) {
+                hrm_run_config c;
+                memset(&c, 0, sizeof(c));
+                c.program_type = HRM_ASYNC;
+                c.variant = SOLO_VARIANT;
+                c.stream = solo_s[lane];
+                c.groups = solo_groups_lane;
+                hrm_run_result r;
+                if (hrm_capi::photon_walk_lane(lane, mu.data(), mu.data(), sp.data(), 2, 1, 0, 0, (uint64_t*)t.data(),
+                                               &c, &r) != HRM_OK)
+                    throw std::runtime_error(std::string("solo lane warm-up: ") + hrm_last_error());
+            }
         }
     }
 
     void release_host_resources() {
         if (exec_s) cudaStreamDestroy(exec_s);
         if (submit_s) cudaStreamDestroy(submit_s);
-        if (solo_s) cudaStreamDestroy(solo_s);
-        solo_s = nullptr;
+        for (auto& st : solo_s) {
+            if (st) cudaStreamDestroy(st);
+            st = nullptr;
+        }
         if (done_host) cudaFreeHost(done_host);
         if (staging) cudaFreeHost(staging);
         if (pinned_ctr) cudaFreeHost(pinned_ctr);
@@ -608,7 +629,9 @@ struct Server : ServerBase {
             solo_exit = true;
         }
         solo_cv.notify_all();
-        if (solo_runner.joinable()) solo_runner.join();
+        for (auto& t : solo_runners)
+            if (t.joinable()) t.join();
+        solo_runners.clear();
     }
 
     void halt_resident() {
@@ -618,19 +641,21 @@ struct Server : ServerBase {
         ck(cudaStreamSynchronize(submit_s), "halt");
     }
 
-    // One solo job on the solo stream: beside the shared resident exec (groups = solo_groups)
-    // or alone on the GPU (groups = 0: every team that fits).
-    void run_solo(unsigned int j, const hrm_job& jb, size_t groups_) {
+    // One solo job on lane `lane`: beside the shared resident exec or with the resident kernel
+    // off the GPU, with the whole share (`whole`: no other solo job is running or waiting) or
+    // a lane's share.
+    void run_solo(unsigned int lane, unsigned int j, const hrm_job& jb, bool alone, bool whole) {
         hrm_run_config c;
         memset(&c, 0, sizeof(c));
         c.program_type = HRM_ASYNC;
         c.variant = SOLO_VARIANT;
-        c.stream = solo_s;
-        c.groups = groups_;
+        c.stream = solo_s[lane];
+        c.groups = alone ? (whole ? alone_groups : alone_groups_lane) : (whole ? solo_groups : solo_groups_lane);
         hrm_run_result r;
-        trace("solo job %u (%u photons) starts %s", j, jb.count, groups_ ? "beside the resident kernel" : "alone");
-        if (hrm_photon_run_device((const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n, jb.seed,
-                                  jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
+        trace("solo job %u (%u photons) starts on lane %u %s, %zu teams", j, jb.count, lane,
+              alone ? "with the resident kernel off the GPU" : "beside the resident kernel", (size_t)c.groups);
+        if (hrm_capi::photon_walk_lane(lane, (const float*)jb.a, (const float*)jb.b, (const uint8_t*)jb.c, jb.n,
+                                       jb.seed, jb.first, jb.count, (uint64_t*)jb.out, &c, &r) != HRM_OK)
             throw std::runtime_error(std::string("solo photon job: ") + hrm_last_error());
         trace("solo job %u ends: %.3f ms on the device, %u execs", j, r.device_ms, r.execs);
         // The run above synchronised with its stream: stamp the completion from the host.
@@ -650,15 +675,16 @@ struct Server : ServerBase {
         return resident_jobs > resident_done ? resident_jobs - resident_done : 0u;
     }
 
-    // The solo runner: serves the solo queue in submission order, one job at a time. With no
-    // job in flight in the resident kernel, a solo job takes the whole GPU (the resident exec
-    // is halted and not relaunched until the job ends; jobs submitted meanwhile wait in the
-    // table); otherwise it runs beside the resident exec once that holds only its share.
-    void solo_loop() {
+    // A solo runner (one per lane): serves the solo queue in submission order, one job at a
+    // time per lane. With no job in flight in the resident kernel, a job runs with the resident
+    // kernel off the GPU (the resident exec is halted and not relaunched while such a job
+    // runs; jobs submitted meanwhile wait in the table); otherwise beside the resident exec
+    // once that holds only its share.
+    void solo_loop(unsigned int lane) {
         try {
             while (true) {
                 std::pair<unsigned int, hrm_job> sj;
-                bool alone = false, halt = false;
+                bool alone = false, halt = false, whole = false;
                 {
                     std::unique_lock<std::mutex> g(solo_lock);
                     solo_cv.wait_for(g, std::chrono::milliseconds(2),
@@ -680,8 +706,11 @@ struct Server : ServerBase {
                     if (!alone && !(exec_shared || !exec_on_gpu)) continue;  // wait for the shared exec
                     sj = solo_queue.front();
                     solo_queue.pop_front();
-                    solo_running = true;
-                    solo_full = alone;
+                    // By itself: the whole share. (A job that starts later with a lane's share
+                    // waits for room until this one ends.)
+                    whole = solo_active == 0 && solo_queue.empty();
+                    solo_active++;
+                    if (alone) solo_alone++;
                 }
                 if (alone) {
                     bool running;
@@ -692,19 +721,23 @@ struct Server : ServerBase {
                     if (running) halt_resident();
                     std::unique_lock<std::mutex> g(solo_lock);
                     solo_cv.wait(g, [this] { return !exec_on_gpu || solo_exit; });
-                    if (solo_exit) break;
+                    if (solo_exit) {
+                        solo_alone--;
+                        solo_active--;
+                        break;
+                    }
                 }
-                run_solo(sj.first, sj.second, alone ? 0u : solo_groups);
+                run_solo(lane, sj.first, sj.second, alone, whole);
                 bool drained;
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
-                    solo_running = false;
-                    solo_full = false;
+                    solo_active--;
+                    if (alone) solo_alone--;
                     solo_done++;
-                    drained = solo_queue.empty() && exec_on_gpu && exec_shared;
+                    drained = solo_queue.empty() && solo_active == 0 && exec_on_gpu && exec_shared;
                 }
                 solo_cv.notify_all();
-                // Nothing left for the solo lane: give the resident exec all its teams back.
+                // Nothing left for the solo lanes: give the resident exec all its teams back.
                 if (drained) halt_resident();
             }
         } catch (std::exception& e) {
@@ -713,7 +746,7 @@ struct Server : ServerBase {
                 err = e.what();
             }
             std::lock_guard<std::mutex> g(solo_lock);
-            solo_full = false;  // never leave the resident loop waiting
+            solo_alone = 0;  // never leave the resident loop waiting
             solo_cv.notify_all();
         }
     }
@@ -735,9 +768,9 @@ struct Server : ServerBase {
                 {
                     // A solo job that holds the whole GPU keeps the resident kernel off it.
                     std::unique_lock<std::mutex> g(solo_lock);
-                    solo_cv.wait(g, [this] { return !solo_full || stop; });
+                    solo_cv.wait(g, [this] { return solo_alone == 0 || stop; });
                     if (stop) break;
-                    shared = solo_photons && (!solo_queue.empty() || solo_running);
+                    shared = solo_photons && (!solo_queue.empty() || solo_active > 0);
                     exec_shared = shared;
                     exec_on_gpu = true;
                     exec_epoch++;
@@ -763,7 +796,7 @@ struct Server : ServerBase {
                 bool solo_left;
                 {
                     std::lock_guard<std::mutex> g(solo_lock);
-                    solo_left = !solo_queue.empty() || solo_running;
+                    solo_left = !solo_queue.empty() || solo_active > 0;
                 }
                 if (!host_open && (f & hrm_rt::COMPLETION_FLAG) && !solo_left) break;
             }
