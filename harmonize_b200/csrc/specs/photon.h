@@ -199,9 +199,12 @@ struct PhotonMove {
         const float face = (float)(up ? c + 1u : c);
         const bool out = up ? (c + 1u == n) : (c == 0u);
         const unsigned int c_next = up ? c + 1u : c - 1u;
-        if (axis == 0) { p.x = face; ix = c_next; }
-        else if (axis == 1) { p.y = face; iy = c_next; }
-        else { p.z = face; iz = c_next; }
+        p.x = axis == 0 ? face : p.x;
+        p.y = axis == 1 ? face : p.y;
+        p.z = axis == 2 ? face : p.z;
+        ix = axis == 0 ? c_next : ix;
+        iy = axis == 1 ? c_next : iy;
+        iz = axis == 2 ? c_next : iz;
         if (out) {
             prog.template async<PhotonTally>(tally_word(n * n * n + (p.id_lo & (PHOTON_SPREAD - 1u)), to_fixed(p.w)));
             return;
