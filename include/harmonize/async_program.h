@@ -947,6 +947,7 @@ class AsyncProgram {
         unsigned int prev_c = 0;          // lane f: f's count at the previous step
         unsigned int age = 0;             // lane f: steps f has held a partial batch that did not grow
         unsigned int rotate = 0;          // next function to favour for a forced partial batch
+        unsigned int quiet = 0;           // partial batches left to run without looking at the arena
         bool quiescent = false;
         const unsigned int my_ring = (lane < FN) ? ring_slots_of(lane) : 0u;  // lane f: f's ring size
         const unsigned int my_group = (lane < FN) ? group_of_fn(lane) : NO_GROUP;  // lane f: f's ring group
@@ -1004,7 +1005,12 @@ class AsyncProgram {
                 if (lane == bf) age = 0;
                 forced = true;
             }
-            if (bc < 32u && !forced) {
+            // A tail: the last look found the arena empty and make_work done, so the next few
+            // partial batches run without another look (each look is a round trip to L2):
+            // Collatz 1..2^20 1.83 -> 1.75 ms, R-MAT 2^22 2.80 -> 2.72 ms, same outputs.
+            const bool tail = bc > 0u && quiet > 0u && !can_make_work;
+            if (tail) quiet--;
+            if (bc < 32u && !forced && !tail) {
                 // No full batch locally: try the arena for the function closest to full.
                 unsigned int av = 0;
                 if (lane < FN) av = hrm_rt::ld_relaxed(&_dev_ctx.rings.heads[lane].avail);
@@ -1065,6 +1071,7 @@ class AsyncProgram {
                     // polling for jobs, must not starve promises already in the stash).
                     if (after != before || bc == 0) continue;
                 }
+                if (fbest == 0 && !can_make_work) quiet = 3;
                 if (bc == 0) {
                     // Nothing local, nothing in the arena, nothing to make: idle.
                     hrm_rt::call_on_idle<PROGRAM_SPEC>(*this);
