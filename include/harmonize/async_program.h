@@ -207,8 +207,8 @@ class AsyncProgram {
         unsigned int held_f[HELD_MAX];  // their functions
         // The team's statistics of this exec, kept here rather than in registers (lane 0
         // updates them) and added to the device counters when the team leaves.
-        // Evaluations are counted per function in fn_evals.
-        unsigned long long n_batches, n_full, n_spill, n_fill, n_mw, n_idle;
+        // Evaluations are counted per function in fn_evals; full batches are n_batches - n_partial.
+        unsigned long long n_batches, n_partial, n_spill, n_fill, n_mw, n_idle;
         unsigned long long fn_evals[FN];
         unsigned int words[RING_WORDS];
     };
@@ -920,7 +920,7 @@ class AsyncProgram {
             _grp_ctx.loads_pending = 0;
             _grp_ctx.overflowed = 0;
             _grp_ctx.n_batches = 0;
-            _grp_ctx.n_full = 0;
+            _grp_ctx.n_partial = 0;
             _grp_ctx.n_spill = 0;
             _grp_ctx.n_fill = 0;
             _grp_ctx.n_mw = 0;
@@ -1115,7 +1115,7 @@ class AsyncProgram {
                 settle_overflow();
                 if (lane == 0) {
                     g.n_batches += 1ull;
-                    g.n_full += (k == 32u);
+                    if (k < 32u) g.n_partial += 1ull;
                     g.fn_evals[bf] += k;
                 }
                 if (k < 32u || forced || rep + 1u >= BURST) break;
@@ -1154,7 +1154,7 @@ class AsyncProgram {
             unsigned long long* st = _dev_ctx.stats;
             atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);
             atomicAdd(&st[hrm_rt::STAT_BATCHES], g.n_batches);
-            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_full);
+            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_batches - g.n_partial);
             atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], g.n_spill);
             atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], g.n_fill);
             atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], g.n_mw);
