@@ -219,7 +219,7 @@ def flush_l2(buf):
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one exec launch on a
 # small case of the same kernel, with its call count: scaled by calls to the bench's launch
 # (profiles/photon_walk_async_exec_kernel_ncu.txt: 10^6 photons, variant 7).
-TRAFFIC_PROFILE = {("photon", "async"): (48791040 + 608079872, 1613907450)}
+TRAFFIC_PROFILE = {("photon", "async"): (47579904 + 609037056, 1613907450)}
 
 BYTES_PER_CALL = {
     "photon": [93, 68, 32],
