@@ -47,3 +47,15 @@ static_assert(!fn_OLDEST_FIRST<Mix42, Job<PhotonMove>>::value && !fn_OLDEST_FIRS
 // Discriminants are 0-based positions in the OpUnion, as in the original runtime.
 static_assert(OpUnionLookup<PhotonTally, PhotonSpec<4, 2>::OpSet>::DISC == 2, "DISC = position");
 static_assert(OpUnionLookup<Job<BfsExpand>, Mix42::OpSet>::DISC == 6, "DISC = position");
+
+// Promises are moved as packed 32-bit words: arguments end to end in call order, each rounded
+// up to whole words, with no alignment padding between them.
+static_assert(Promise<CollatzEven>::WORDS == 4, "(u64, u32, u32): 4 words");
+static_assert(Promise<PhotonMove>::WORDS == 11, "a moving photon: 11 words");
+static_assert(Promise<PhotonCollide>::WORDS == 8, "a photon at a collision: 8 words (no direction)");
+static_assert(Promise<PhotonTally>::WORDS == 2, "a tally: one 64-bit word");
+static_assert(Promise<BfsRelax>::WORDS == 2 && Promise<BfsExpand>::WORDS == 4, "BFS: 2 and 4 words");
+static_assert(Promise<Job<CollatzEven>>::WORDS == 5, "(u32 job, u64, u32, u32): 5 words, not the 6 of its ArgTuple");
+static_assert(Promise<Job<PhotonTally>>::WORDS == 3, "(u32 job, u64): 3 words");
+static_assert(ArgWordOffset<1, Promise<Job<CollatzEven>>::Args>::value == 1, "the u64 right after the job id");
+static_assert(ArgWordOffset<3, Promise<Job<CollatzEven>>::Args>::value == 4, "last argument at word 4");
