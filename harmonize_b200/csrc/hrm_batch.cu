@@ -1305,6 +1305,10 @@ int hrm_solo_run(const hrm_job* jobs, uint32_t njobs, int variant, uint32_t nlan
             validate(jobs[j]);
             if (jobs[j].kind != HRM_JOB_PHOTON) throw std::invalid_argument("hrm_solo_run takes photon jobs only");
         }
+        if (njobs == 0) {
+            if (total_ms) *total_ms = 0.0f;
+            return HRM_OK;
+        }
         int dev = 0;
         ck(cudaGetDevice(&dev), "cudaGetDevice");
         const size_t teams = hrm_capi::photon_resident_teams(variant);
