@@ -55,8 +55,9 @@ class RunConfig(ctypes.Structure):
 
 # Compiled tuning variants: (shared-memory ring links per function, teams per CTA). The lean
 # variants (5, 6) give the first function 4 links and the others 2 and are compiled for at
-# least 10 / 11 resident CTAs per SM; 7 and 8 are R4/T2 and R4/T4 compiled for at least 11 / 5.
-VARIANTS = {0: (2, 4), 1: (4, 4), 2: (4, 2), 3: (8, 2), 4: (2, 8), 5: (4, 2), 6: (4, 2), 7: (4, 2), 8: (4, 4)}
+# least 10 / 11 resident CTAs per SM; 7 and 8 are R4/T2 and R4/T4 compiled for at least 11 / 5;
+# 9 is R3/T2 (3-link rings) compiled for at least 14.
+VARIANTS = {0: (2, 4), 1: (4, 4), 2: (4, 2), 3: (8, 2), 4: (2, 8), 5: (4, 2), 6: (4, 2), 7: (4, 2), 8: (4, 4), 9: (3, 2)}
 
 
 class RunResult(ctypes.Structure):

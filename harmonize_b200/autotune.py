@@ -64,7 +64,7 @@ def _single_spec_workloads():
 
 def _candidates(prog, variants):
     if prog == "event":  # EventProgram has no rings and no arena fills: teams per CTA only
-        return [dict(variant=v) for v in variants if v not in (1, 3, 5, 6, 7, 8)]
+        return [dict(variant=v) for v in variants if v not in (1, 3, 5, 6, 7, 8, 9)]
     return [dict(variant=v, patience=p, fill_links=f) for v, p, f in itertools.product(variants, PATIENCE, FILL_LINKS)]
 
 

@@ -137,6 +137,7 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_LEAN_T2_M11: return new ProgramImpl<AsyncProgram<LeanRings<SPEC<4, 2>, 4, 2, 11>>>(arena, s);
             case HRM_VARIANT_R4_T2_M11: return new ProgramImpl<AsyncProgram<MinCtas<SPEC<4, 2>, 11>>>(arena, s);
             case HRM_VARIANT_R4_T4_M5: return new ProgramImpl<AsyncProgram<MinCtas<SPEC<4, 4>, 5>>>(arena, s);
+            case HRM_VARIANT_R3_T2_M14: return new ProgramImpl<AsyncProgram<MinCtas<SPEC<3, 2>, 14>>>(arena, s);
             default: break;
         }
     } else if (type == HRM_EVENT) {
@@ -147,7 +148,8 @@ ProgramBase* make_variant(int type, int variant, size_t arena, const STATE& s) {
             case HRM_VARIANT_R8_T2:
             case HRM_VARIANT_LEAN_T2_M10:
             case HRM_VARIANT_LEAN_T2_M11:
-            case HRM_VARIANT_R4_T2_M11: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
+            case HRM_VARIANT_R4_T2_M11:
+            case HRM_VARIANT_R3_T2_M14: return new ProgramImpl<EventProgram<SPEC<2, 2>>>(arena, s);
             case HRM_VARIANT_R4_T4_M5: return new ProgramImpl<EventProgram<SPEC<2, 4>>>(arena, s);
             case HRM_VARIANT_R2_T8: return new ProgramImpl<EventProgram<SPEC<2, 8>>>(arena, s);
             default: break;

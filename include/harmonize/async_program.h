@@ -77,7 +77,7 @@ class AsyncProgram {
 
     static const unsigned int RING_LINKS = (unsigned int)hrm_rt::spec_RING_LINKS<PROGRAM_SPEC>::value;
     static const unsigned int RING = RING_LINKS * 32u;
-    static_assert(RING_LINKS >= 2 && (RING & (RING - 1)) == 0, "RING_LINKS must be a power of two >= 2");
+    static_assert(RING_LINKS >= 2, "RING_LINKS must be at least 2");
     static const unsigned int TEAMS_PER_CTA = (unsigned int)hrm_rt::spec_TEAMS_PER_CTA<PROGRAM_SPEC>::value;
     static const unsigned int CTA_THREADS = TEAMS_PER_CTA * 32u;
     static const unsigned int MIN_CTAS_PER_SM = (unsigned int)hrm_rt::spec_MIN_CTAS_PER_SM<PROGRAM_SPEC>::value;
@@ -156,13 +156,24 @@ class AsyncProgram {
     __host__ __device__ static constexpr bool rings_valid() {
         if constexpr (I < FN) {
             constexpr unsigned int s = ring_slots<I>();
-            return s >= 64u && (s & (s - 1u)) == 0u && rings_valid<I + 1>();
+            return s >= 64u && s % 32u == 0u && rings_valid<I + 1>();
         } else {
             return true;
         }
     }
-    static_assert(rings_valid<0>(), "ring sizes must be powers of two of at least 2 links");
+    static_assert(rings_valid<0>(), "rings hold at least 2 links");
     static const unsigned int RING_WORDS = max_group_words<0>();
+    // Ring index a (a < 2 * SLOTS: a ring position < SLOTS plus an offset <= SLOTS) reduced
+    // to a slot. A mask for power-of-two rings, one compare and subtract for the others
+    // (e.g. 3 links, so that a team's stash is smaller and more teams fit on an SM).
+    template <unsigned int SLOTS>
+    __host__ __device__ static constexpr unsigned int wrap_slot(unsigned int a) {
+        if constexpr ((SLOTS & (SLOTS - 1u)) == 0u) {
+            return a & (SLOTS - 1u);
+        } else {
+            return a >= SLOTS ? a - SLOTS : a;
+        }
+    }
     // Ring size and ring group of function f (run-time f).
     template <unsigned int I = 0>
     __device__ static __forceinline__ unsigned int ring_slots_of(unsigned int f) {
@@ -479,7 +490,7 @@ class AsyncProgram {
         const unsigned int idx = base + rank;
         const unsigned int over = __ballot_sync(mask, idx >= SLOTS);
         if (idx < SLOTS) {
-            const unsigned int slot = (g.bottom[F] + idx) & (SLOTS - 1);
+            const unsigned int slot = wrap_slot<SLOTS>(g.bottom[F] + idx);
 #pragma unroll
             for (unsigned int i = 0; i < W; i++) g.words[BASE + i * SLOTS + slot] = w[i];
         }
@@ -546,7 +557,7 @@ class AsyncProgram {
         }
         const unsigned int over = __ballot_sync(mask, idx >= SLOTS);
         if (idx < SLOTS) {
-            const unsigned int slot = (g.bottom[F] + idx) & (SLOTS - 1);
+            const unsigned int slot = wrap_slot<SLOTS>(g.bottom[F] + idx);
 #pragma unroll
             for (unsigned int i = 0; i < W; i++) {
                 unsigned int* dst = &g.words[BASE + i * SLOTS + slot];
@@ -721,7 +732,7 @@ class AsyncProgram {
             unsigned int dst = __shfl_sync(0xFFFFFFFFu, link, l);
             unsigned int k = l * 32u + lane;
             if (k < n) {
-                unsigned int slot = (bottom + k) & (SLOTS - 1);
+                unsigned int slot = wrap_slot<SLOTS>(bottom + k);
 #pragma unroll
                 for (unsigned int i = 0; i < W; i++) __stcg(link_word_ptr(dst, i, lane), g.words[BASE + i * SLOTS + slot]);
             }
@@ -731,7 +742,7 @@ class AsyncProgram {
         hrm_rt::ring_push(_dev_ctx.rings, _dev_ctx.ctl, F, hrm_rt::encode_link(link, cnt_l), lane, nl, 0xFFFFFFFFu);
         __syncwarp();
         if (lane == 0) {
-            g.bottom[F] = (bottom + n) & (SLOTS - 1);
+            g.bottom[F] = wrap_slot<SLOTS>(bottom + n);
             g.count[F] = cnt - n;
         }
         __syncwarp();
@@ -781,7 +792,7 @@ class AsyncProgram {
             unsigned int src = hrm_rt::entry_link(el);
             unsigned int k = hrm_rt::entry_count(el);
             if (lane < k) {
-                unsigned int slot = (bottom + cnt + lane) & (SLOTS - 1);
+                unsigned int slot = wrap_slot<SLOTS>(bottom + cnt + lane);
 #pragma unroll
                 for (unsigned int i = 0; i < W; i++) g.words[BASE + i * SLOTS + slot] = __ldcg(link_word_ptr(src, i, lane));
             }
@@ -825,7 +836,7 @@ class AsyncProgram {
             unsigned int w[W];
             // The k newest promises (top of the ring), or the k oldest (bottom) for functions
             // whose spec asks for OLDEST_FIRST; the batch's calls are appended at the top.
-            unsigned int slot = ((OLDEST_FIRST ? bottom : bottom + cnt - k) + lane) & (SLOTS - 1);
+            unsigned int slot = wrap_slot<SLOTS>((OLDEST_FIRST ? bottom : bottom + cnt - k) + lane);
 #pragma unroll
             for (unsigned int i = 0; i < W; i++) w[i] = g.words[BASE + i * SLOTS + slot];
             p.from_words(w);
@@ -833,7 +844,7 @@ class AsyncProgram {
         __syncwarp();
         if (lane == 0) {
             g.count[F] = cnt - k;
-            if (OLDEST_FIRST) g.bottom[F] = (bottom + k) & (SLOTS - 1);
+            if (OLDEST_FIRST) g.bottom[F] = wrap_slot<SLOTS>(bottom + k);
         }
         __syncwarp();
         if (lane < k) {
@@ -938,6 +949,7 @@ class AsyncProgram {
         hrm_rt::call_initialize<PROGRAM_SPEC>(*this);
         __syncwarp();
         publish_held();
+        clamp_counts();  // pushes past a ring went to the arena
 
         GroupContext& g = _grp_ctx;
         hrm_rt::RuntimeControl* ctl = _dev_ctx.ctl;
@@ -1128,6 +1140,7 @@ class AsyncProgram {
         hrm_rt::call_finalize<PROGRAM_SPEC>(*this);
         __syncwarp();
         publish_held();
+        clamp_counts();  // pushes past a ring went to the arena
         hrm_rt::call_before_publish<PROGRAM_SPEC>(*this);
         __syncwarp();
 

@@ -70,7 +70,7 @@ HRM_SPEC_CONST(OLDEST_FIRST, 0)
 
 // Per-function ring size: a spec may give functions rings of different sizes by defining
 //   template <typename Op> struct RING_LINKS_OF { static const size_t value = ...; };
-// (a power of two >= 2 for each Op); otherwise every function gets RING_LINKS.
+// (at least 2 for each Op); otherwise every function gets RING_LINKS.
 template <class S, class Op, class = void>
 struct fn_RING_LINKS : spec_RING_LINKS<S> {};
 template <class S, class Op>

@@ -109,7 +109,11 @@ typedef struct hrm_run_config {
  * limit on teams per SM). */
 #define HRM_VARIANT_R4_T2_M11 7
 #define HRM_VARIANT_R4_T4_M5 8
-#define HRM_VARIANT_COUNT 9
+/* 3-link rings (the photon walk's Collide 2), 2 teams per CTA, compiled for at least 14 resident
+ * CTAs per SM: a stash small enough for 14 CTAs of 2 teams in an SM's shared memory, and at most
+ * 72 registers a thread so that 7 teams fit each SM sub-partition (28 warps per SM). */
+#define HRM_VARIANT_R3_T2_M14 9
+#define HRM_VARIANT_COUNT 10
 
 /* What a whole run reports back. */
 typedef struct hrm_run_result {

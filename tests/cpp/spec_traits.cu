@@ -59,3 +59,13 @@ static_assert(Promise<Job<CollatzEven>>::WORDS == 5, "(u32 job, u64, u32, u32): 
 static_assert(Promise<Job<PhotonTally>>::WORDS == 3, "(u32 job, u64): 3 words");
 static_assert(ArgWordOffset<1, Promise<Job<CollatzEven>>::Args>::value == 1, "the u64 right after the job id");
 static_assert(ArgWordOffset<3, Promise<Job<CollatzEven>>::Args>::value == 4, "last argument at word 4");
+
+// Team rings need not be powers of two: a 3-link photon spec (Collide 2 links) has 96-slot Move
+// and Tally rings, and ring positions wrap by one subtraction below 2 * SLOTS.
+using Photon3 = AsyncProgram<PhotonSpec<3, 2>>;
+static_assert(Photon3::ring_slots<0>() == 96 && Photon3::ring_slots<1>() == 64 && Photon3::ring_slots<2>() == 96,
+              "3-link rings: Move 96, Collide 64, Tally 96 slots");
+static_assert(Photon3::RING_WORDS == 96 * 11 + 64 * 8 + 96 * 2, "stash words of the 3-link photon spec");
+static_assert(Photon3::wrap_slot<96>(95) == 95 && Photon3::wrap_slot<96>(96) == 0 && Photon3::wrap_slot<96>(191) == 95,
+              "96-slot ring wraps at 96");
+static_assert(Photon3::wrap_slot<128>(200) == 72 && Photon3::wrap_slot<64>(64) == 0, "power-of-two rings mask");
