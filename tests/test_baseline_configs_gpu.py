@@ -5,7 +5,8 @@
   * BFS levels of the R-MAT 2^22 graph, edge factor 16, (a, b, c) = (0.57, 0.19, 0.19), seed 1,
     from vertex 0, both program types, against the serial BFS;
   * the photon walk on the 128^3 bench medium (medium seed 2024, walk seed 0x5EED0123456789),
-    10^6 photons, both program types, against the OpenMP host executor of the same spec.
+    10^6 photons, both program types (AsyncProgram in three tuning variants), against the OpenMP
+    host executor of the same spec.
 Every output is compared bit for bit; call counts are compared where they are a pure function
 of the inputs (Collatz, photon walk)."""
 import numpy as np
@@ -50,10 +51,12 @@ def photon128(hrm):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("program", ["async", "event"])
-def test_photon_bench_medium(hrm, photon128, program):
+@pytest.mark.parametrize("program,variant", [("async", 0), ("event", 0), ("async", 7), ("async", 9)])
+def test_photon_bench_medium(hrm, photon128, program, variant):
+    """Variant 7 is the tuned one; variant 9's 3-link rings spill and refill links of moves on
+    most steps, so every wrapped ring position of the spill and fill paths is exercised."""
     mu, ab, sp, count, ref, calls = photon128
-    tally, res = hrm.photon_walk(mu, ab, sp, 128, BENCH_SEED, 0, count, program=program)
+    tally, res = hrm.photon_walk(mu, ab, sp, 128, BENCH_SEED, 0, count, program=program, variant=variant)
     assert np.array_equal(tally, ref), f"{int((tally != ref).sum())} tally slots differ"
     assert res["evals"] == int(calls.sum())
     for f in range(3):
