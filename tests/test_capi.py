@@ -26,6 +26,19 @@ def test_header_declares_the_life_cycle():
         assert n in names
 
 
+def test_variant_table_matches_the_header(hrm):
+    """Every HRM_VARIANT_* the header defines, and no other, has a (ring links, teams per CTA)
+    entry in the package's variant table, and the ring and team counts in each name agree."""
+    text = open(HEADER).read()
+    defined = dict((n, int(v)) for n, v in re.findall(r"#define HRM_VARIANT_(\w+) (\d+)", text))
+    count = defined.pop("COUNT")
+    assert sorted(defined.values()) == list(range(count)) == sorted(hrm.VARIANTS)
+    for name, v in defined.items():
+        m = re.match(r"R(\d+)_T(\d+)", name)
+        if m:
+            assert hrm.VARIANTS[v] == (int(m.group(1)), int(m.group(2))), name
+
+
 def test_library_exports_every_declared_symbol(hrm):
     lib = ctypes.CDLL(hrm.LIB_PATH)
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
