@@ -218,8 +218,9 @@ class AsyncProgram {
         unsigned int held_f[HELD_MAX];  // their functions
         // The team's statistics of this exec, kept here rather than in registers (lane 0
         // updates them) and added to the device counters when the team leaves.
-        // Evaluations are counted per function in fn_evals; full batches are n_batches - n_partial.
-        unsigned long long n_batches, n_partial, n_spill, n_fill, n_mw, n_idle;
+        // Evaluations are counted per function in fn_evals; partial batches and their evaluations
+        // in n_partial and partial_evals, so full batches are (evals - partial_evals) / 32.
+        unsigned long long partial_evals, n_partial, n_spill, n_fill, n_mw, n_idle;
         unsigned long long fn_evals[FN];
         unsigned int words[RING_WORDS];
     };
@@ -818,9 +819,12 @@ class AsyncProgram {
         }
     }
 
-    // Pops the newest k promises of function F and evaluates them, one per lane.
+    // Pops the newest k promises of function F and evaluates them, one per lane. `cnt` is F's
+    // count as the scheduler read it (every lane read it before the warp-wide steps that chose
+    // the batch, so lane 0 may overwrite it without another barrier); lane 0 also counts the
+    // batch in the team's statistics.
     template <unsigned int F>
-    __device__ __forceinline__ void run_typed(unsigned int k) {
+    __device__ __forceinline__ void run_typed(unsigned int k, unsigned int cnt) {
         using Op = typename OpAt<F, OpSet>::type;
         constexpr unsigned int W = Promise<Op>::WORDS;
         constexpr unsigned int SLOTS = ring_slots<F>();
@@ -829,7 +833,6 @@ class AsyncProgram {
         GroupContext& g = _grp_ctx;
         const unsigned int lane = util::lane_id();
         settle_loads();
-        const unsigned int cnt = g.count[F];
         const unsigned int bottom = g.bottom[F];
         Promise<Op> p;
         if (lane < k) {
@@ -841,10 +844,15 @@ class AsyncProgram {
             for (unsigned int i = 0; i < W; i++) w[i] = g.words[BASE + i * SLOTS + slot];
             p.from_words(w);
         }
-        __syncwarp();
+        if constexpr (OLDEST_FIRST) __syncwarp();  // every lane has read bottom before lane 0 moves it
         if (lane == 0) {
             g.count[F] = cnt - k;
             if (OLDEST_FIRST) g.bottom[F] = wrap_slot<SLOTS>(bottom + k);
+            g.fn_evals[F] += k;
+            if (k < 32u) {
+                g.n_partial += 1ull;
+                g.partial_evals += k;
+            }
         }
         __syncwarp();
         if (lane < k) {
@@ -854,18 +862,19 @@ class AsyncProgram {
     }
 
     template <unsigned int I>
-    __device__ __forceinline__ void run_fn(unsigned int f, unsigned int k) {
+    __device__ __forceinline__ void run_fn(unsigned int f, unsigned int k, unsigned int cnt) {
         if constexpr (I < FN) {
-            if (f == I) run_typed<I>(k);
-            else run_fn<I + 1>(f, k);
+            if (f == I) run_typed<I>(k, cnt);
+            else run_fn<I + 1>(f, k, cnt);
         }
     }
 
     // Whole team, after a batch: publishes the arena links of the promises that did not fit in
     // the rings during the batch and clamps the counts. When no push overflowed (the common
     // case) this is one shared-memory read.
+    template <bool SYNCED = false>
     __device__ __forceinline__ void settle_overflow() {
-        __syncwarp();
+        if constexpr (!SYNCED) __syncwarp();
         if (*(volatile unsigned int*)&_grp_ctx.overflowed == 0u) return;
         __syncwarp();
         if (util::lane_id() == 0) _grp_ctx.overflowed = 0u;
@@ -930,7 +939,7 @@ class AsyncProgram {
             _grp_ctx.held_n = 0;
             _grp_ctx.loads_pending = 0;
             _grp_ctx.overflowed = 0;
-            _grp_ctx.n_batches = 0;
+            _grp_ctx.partial_evals = 0;
             _grp_ctx.n_partial = 0;
             _grp_ctx.n_spill = 0;
             _grp_ctx.n_fill = 0;
@@ -1044,6 +1053,9 @@ class AsyncProgram {
                             if (cf > 0) spill_fn<0>(f, (cf + 31u) / 32u);
                         }
                         if (__all_sync(0xFFFFFFFFu, lane >= FN || g.count[lane] == 0u)) continue;
+                        // A full arena kept some promises here: go on with the counts as they are.
+                        c = (lane < FN) ? g.count[lane] : 0u;
+                        bc = __shfl_sync(0xFFFFFFFFu, c, bf);
                     }
                 }
                 if (fbest != 0) {
@@ -1122,17 +1134,17 @@ class AsyncProgram {
             // keeps a batch's worth of room, up to BURST - 1 more batches of it without a
             // scheduling step (one evaluation site, so the kernel holds one copy of each eval).
             for (unsigned int rep = 0;; rep++) {
-                run_fn<0>(bf, k);
-                hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
-                settle_overflow();
-                if (lane == 0) {
-                    g.n_batches += 1ull;
-                    if (k < 32u) g.n_partial += 1ull;
-                    g.fn_evals[bf] += k;
+                run_fn<0>(bf, k, bc);
+                if constexpr (hrm_rt::has_after_batch<PROGRAM_SPEC, ProgramType>::value) {
+                    hrm_rt::call_after_batch<PROGRAM_SPEC>(*this);
+                    settle_overflow();
+                } else {
+                    settle_overflow<true>();  // run_fn ended with a barrier
                 }
                 if (k < 32u || forced || rep + 1u >= BURST) break;
                 const unsigned int cn = (lane < FN) ? g.count[lane] : 0u;
-                if (__shfl_sync(0xFFFFFFFFu, cn, bf) < 32u) break;
+                bc = __shfl_sync(0xFFFFFFFFu, cn, bf);
+                if (bc < 32u) break;
                 if (__any_sync(0xFFFFFFFFu, lane < FN && lane != bf && cn + 32u > my_ring)) break;
             }
         }
@@ -1166,8 +1178,9 @@ class AsyncProgram {
             }
             unsigned long long* st = _dev_ctx.stats;
             atomicAdd(&st[hrm_rt::STAT_EVALS], n_evals);
-            atomicAdd(&st[hrm_rt::STAT_BATCHES], g.n_batches);
-            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], g.n_batches - g.n_partial);
+            const unsigned long long full = (n_evals - g.partial_evals) / 32ull;
+            atomicAdd(&st[hrm_rt::STAT_BATCHES], full + g.n_partial);
+            atomicAdd(&st[hrm_rt::STAT_FULL_BATCHES], full);
             atomicAdd(&st[hrm_rt::STAT_SPILL_LINKS], g.n_spill);
             atomicAdd(&st[hrm_rt::STAT_FILL_LINKS], g.n_fill);
             atomicAdd(&st[hrm_rt::STAT_MAKE_WORK], g.n_mw);
