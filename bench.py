@@ -298,7 +298,9 @@ def run_photon(args, hrm, rank, world, pg, torch):
             total = ctypes.c_float()
             hrm.check(JL.hrm_plain_run(ctypes.byref(arr), 1, 1, done.ctypes.data, ctypes.byref(total)))
             best = total.value if best is None else min(best, total.value)
-        return best, bool(torch.equal(d_plain, d_tally))
+        return best, {"same_tallies": bool(torch.equal(d_plain, d_tally)),
+                      "what": "one thread per source photon walking its split descendants on a per-thread stack, "
+                              "one launch, best of 3; equivalent calls = the runtime's call count for these photons"}
 
     return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
                 plain_arm=plain_arm,
@@ -387,7 +389,30 @@ def run_collatz(args, hrm, rank, world, pg, torch):
                "sample": "n = 1..2^20, OpenMP host executor of the same spec source"}
         return ok, cpu
 
+    def plain_arm(flush):
+        """The same start values through the plain kernel of the reference's plain Collatz example
+        (examples/cpp/collaz/collaz_std.cpp:5-21: one thread per start value, iterating to 1),
+        best of three with L2 flushed, and whether its step counts equal the timed run's.
+        Outside the timed region."""
+        from harmonize_b200 import jobs
+        d_plain = torch.empty(count, dtype=torch.int32, device="cuda")
+        arr = (jobs.Job * 1)()
+        arr[0] = jobs.Job(jobs.JOB_COLLATZ, start, count, 0, 0, None, None, None, d_plain.data_ptr())
+        JL = jobs._bind()
+        best = None
+        for _ in range(3):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            done = np.zeros(1, dtype=np.uint64)
+            total = ctypes.c_float()
+            hrm.check(JL.hrm_plain_run(ctypes.byref(arr), 1, 1, done.ctypes.data, ctypes.byref(total)))
+            best = total.value if best is None else min(best, total.value)
+        return best, {"same_outputs": bool(torch.equal(d_plain, d_out)),
+                      "what": "one thread per start value iterating to 1, one launch, best of 3; equivalent calls = "
+                              "the runtime's call count for these start values"}
+
     return dict(step_device=step_device, step_e2e=step_e2e, checksum=checksum, oracle_check=oracle_check,
+                plain_arm=plain_arm,
                 h2d=0, d2h=count * 4, dtype="u64",
                 bytes_per_call=BYTES_PER_CALL["collatz"], launches_per_step=3 if args.program == "async" else 2)
 
@@ -576,15 +601,13 @@ def main():
     e2e_calls = sum_over_ranks(pg, st["evals"] * e2e_steps)
     e2e_value = e2e_calls / (e2e_total / 1e3)
 
-    # Rank 0: the plain one-thread-per-photon kernel on the same photons (not a bench arm: the
+    # Rank 0: the plain one-thread-per-item kernel on the same inputs (not a bench arm: the
     # runtime's non-runtime baseline, outside the timed region).
     plain = None
     if rank == 0 and "plain_arm" in wl:
-        p_ms, p_same = wl["plain_arm"](flush)
-        plain = {"ms": round(p_ms, 3), "equivalent_calls_per_s": round(stats_all[-1]["evals"] / (p_ms / 1e3), 1),
-                 "same_tallies": p_same,
-                 "what": "one thread per source photon walking its split descendants on a per-thread stack, "
-                         "one launch, best of 3; equivalent calls = the runtime's call count for these photons"}
+        p_ms, p_info = wl["plain_arm"](flush)
+        plain = dict({"ms": round(p_ms, 3),
+                      "equivalent_calls_per_s": round(stats_all[-1]["evals"] / (p_ms / 1e3), 1)}, **p_info)
 
     pk = peaks()
     s0 = stats_all[-1]

@@ -84,3 +84,41 @@ def test_reference_arm_names_resolve():
     assert names, "no oracle names found"
     missing = [n for n in sorted(names) if not hasattr(oracle, n)]
     assert not missing, missing
+
+
+def test_collatz_plain_leg_passes_the_whole_range_as_one_plain_job(monkeypatch):
+    """The Collatz bench line's plain_kernel leg: one plain job over the bench's start values
+    (1 .. 2^20) through hrm_plain_run on one stream, best of three, its outputs compared with
+    the timed run's. The device is faked here; the leg's C entry point runs in the GPU tests."""
+    import ctypes
+    import types
+
+    import harmonize_b200 as hrm
+    from harmonize_b200 import jobs
+
+    seen = []
+
+    class FakeJobsLib:
+        def hrm_plain_run(self, arr_ref, njobs, nstreams, done_ptr, total_ref):
+            j = arr_ref._obj[0]
+            seen.append((j.kind, j.first, j.count, j.out, njobs, nstreams))
+            total_ref._obj.value = 2.0 + len(seen)  # 3, 4, 5 ms: best of three is 3
+            return 0
+
+    class FakeTensor:
+        def data_ptr(self):
+            return 0x1000
+
+        def pin_memory(self):
+            return self
+
+    fake_torch = types.SimpleNamespace(empty=lambda *a, **k: FakeTensor(), int32="int32",
+                                       equal=lambda a, b: True, cuda=types.SimpleNamespace(synchronize=lambda: None))
+    monkeypatch.setattr(jobs, "_bind", lambda: FakeJobsLib())
+    monkeypatch.setattr(bench, "flush_l2", lambda buf: None)
+    args = types.SimpleNamespace(program="async", variant=2, workload="collatz")
+    wl = bench.run_collatz(args, hrm, 0, 1, None, fake_torch)
+    ms, info = wl["plain_arm"](None)
+    assert ms == 3.0
+    assert info["same_outputs"] is True and "one thread per start value" in info["what"]
+    assert seen == [(jobs.JOB_COLLATZ, 1, 1 << 20, 0x1000, 1, 1)] * 3
