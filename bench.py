@@ -534,6 +534,12 @@ def pick_variant(args, hrm):
     return pick_config(args)["variant"]
 
 
+def plain_record(ms, runtime_calls, info):
+    """The line's plain_kernel entry: the plain kernel's time, the runtime's call count for the
+    same inputs over that time, and the leg's own fields (output comparison, description)."""
+    return dict({"ms": round(ms, 3), "equivalent_calls_per_s": round(runtime_calls / (ms / 1e3), 1)}, **info)
+
+
 def algorithmic_bytes(stats, per_call):
     return sum(stats.get(f"fn{i}_evals", 0) * b for i, b in enumerate(per_call))
 
@@ -606,8 +612,7 @@ def main():
     plain = None
     if rank == 0 and "plain_arm" in wl:
         p_ms, p_info = wl["plain_arm"](flush)
-        plain = dict({"ms": round(p_ms, 3),
-                      "equivalent_calls_per_s": round(stats_all[-1]["evals"] / (p_ms / 1e3), 1)}, **p_info)
+        plain = plain_record(p_ms, stats_all[-1]["evals"], p_info)
 
     pk = peaks()
     s0 = stats_all[-1]

@@ -122,3 +122,50 @@ def test_collatz_plain_leg_passes_the_whole_range_as_one_plain_job(monkeypatch):
     assert ms == 3.0
     assert info["same_outputs"] is True and "one thread per start value" in info["what"]
     assert seen == [(jobs.JOB_COLLATZ, 1, 1 << 20, 0x1000, 1, 1)] * 3
+
+
+def test_photon_plain_leg_passes_the_photons_as_one_plain_job(monkeypatch):
+    """The photon bench line's plain_kernel leg: one plain photon job (the bench's photons and
+    medium) through hrm_plain_run on one stream, best of three, its tallies compared with the
+    timed run's; the leg reports its own description for the line. Device faked, as above."""
+    import types
+
+    import harmonize_b200 as hrm
+    from harmonize_b200 import jobs
+
+    seen = []
+
+    class FakeJobsLib:
+        def hrm_plain_run(self, arr_ref, njobs, nstreams, done_ptr, total_ref):
+            j = arr_ref._obj[0]
+            seen.append((j.kind, j.first, j.count, j.n, j.seed, njobs, nstreams))
+            total_ref._obj.value = 10.0 - len(seen)  # 9, 8, 7 ms: best of three is 7
+            return 0
+
+    class FakeTensor:
+        def data_ptr(self):
+            return 0x2000
+
+        def cuda(self):
+            return self
+
+        def pin_memory(self):
+            return self
+
+    fake_torch = types.SimpleNamespace(from_numpy=lambda a: FakeTensor(), zeros=lambda *a, **k: FakeTensor(),
+                                       int64="int64", equal=lambda a, b: False,
+                                       cuda=types.SimpleNamespace(synchronize=lambda: None))
+    monkeypatch.setattr(jobs, "_bind", lambda: FakeJobsLib())
+    monkeypatch.setattr(bench, "flush_l2", lambda buf: None)
+    args = types.SimpleNamespace(program="async", variant=2, workload="photon", grid=8, photons=100)
+    wl = bench.run_photon(args, hrm, 0, 1, None, fake_torch)
+    ms, info = wl["plain_arm"](None)
+    assert ms == 7.0
+    assert info["same_tallies"] is False and "one thread per source photon" in info["what"]
+    assert seen == [(jobs.JOB_PHOTON, 0, 100, 8, 0x5EED0123456789, 1, 1)] * 3
+
+
+def test_plain_record_of_the_line():
+    rec = bench.plain_record(385.6843, 16119494612, {"same_tallies": True, "what": "w"})
+    assert rec == {"ms": 385.684, "equivalent_calls_per_s": round(16119494612 / 0.3856843, 1),
+                   "same_tallies": True, "what": "w"}
