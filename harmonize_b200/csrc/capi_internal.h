@@ -47,11 +47,37 @@ size_t photon_resident_teams(int variant);
 // `variant` on the current device (HRM_VARIANT_R4_T4_M5 only).
 CtaFootprint photon_cta_footprint(int variant);
 
-// CTAs per SM of kernel B that fit beside `a_ctas` CTAs per SM of kernel A on the current
-// device: shared memory (with the per-CTA reservation), threads, CTA slots, and registers per
-// SM sub-partition (a quarter of the register file; a CTA's warps spread over the four
-// sub-partitions, so a kernel of w warps per CTA at c CTAs takes ceil(c*w/4) warps' registers
-// from each).
+// What one SM offers the CTAs resident on it (B200: 233,472 B of shared memory with 1,024 B
+// reserved per CTA, 65,536 registers in four sub-partitions, 2,048 threads, 32 CTAs).
+struct SmLimits {
+    size_t smem = 0;          // shared memory per SM
+    size_t reserved = 0;      // shared memory reserved by the system per CTA
+    size_t regs = 0;          // registers per SM
+    size_t threads = 0;       // resident threads per SM
+    unsigned int blocks = 0;  // resident CTAs per SM
+};
+
+// CTAs per SM of kernel B (at most 64) that fit beside `a_ctas` CTAs per SM of kernel A on an
+// SM with limits `sm`: shared memory (with the per-CTA reservation), threads, CTA slots, and
+// registers per SM sub-partition (a quarter of the register file; a CTA's warps spread over
+// the four sub-partitions, so a kernel of w warps per CTA at c CTAs takes ceil(c*w/4) warps'
+// registers from each, a warp's registers allocated in units of 256).
+constexpr unsigned int ctas_beside(const CtaFootprint& a, unsigned int a_ctas, const CtaFootprint& b,
+                                   const SmLimits& sm) {
+    const auto warp_regs = [](unsigned int regs) { return (size_t)((regs * 32u + 255u) / 256u) * 256u; };
+    const auto warps = [](const CtaFootprint& f) { return (f.threads + 31u) / 32u; };
+    const size_t part_regs = sm.regs / 4u;
+    for (unsigned int c = 64; c > 0; c--) {
+        const size_t smem = (size_t)a_ctas * (a.smem + sm.reserved) + (size_t)c * (b.smem + sm.reserved);
+        const size_t threads = (size_t)a_ctas * a.threads + (size_t)c * b.threads;
+        const size_t regs = (size_t)((a_ctas * warps(a) + 3u) / 4u) * warp_regs(a.regs_per_thread) +
+                            (size_t)((c * warps(b) + 3u) / 4u) * warp_regs(b.regs_per_thread);
+        if (smem <= sm.smem && threads <= sm.threads && a_ctas + c <= sm.blocks && regs <= part_regs) return c;
+    }
+    return 0;
+}
+
+// The same on the current device.
 unsigned int ctas_beside(const CtaFootprint& a, unsigned int a_ctas, const CtaFootprint& b);
 
 // Two timing events, destroyed on every path out of the scope that made them (a failed

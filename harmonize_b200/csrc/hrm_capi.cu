@@ -494,19 +494,13 @@ unsigned int hrm_capi::ctas_beside(const CtaFootprint& a, unsigned int a_ctas, c
     ck(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev), "attribute");
     ck(cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev), "attribute");
     ck(cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev), "attribute");
-    auto warp_regs = [](unsigned int regs) { return (size_t)((regs * 32u + 255u) / 256u) * 256u; };
-    auto warps = [](const CtaFootprint& f) { return (f.threads + 31u) / 32u; };
-    const size_t part_regs = (size_t)regs_sm / 4u;
-    for (unsigned int c = 64; c > 0; c--) {
-        const size_t smem = (size_t)a_ctas * (a.smem + reserved) + (size_t)c * (b.smem + reserved);
-        const size_t threads = (size_t)a_ctas * a.threads + (size_t)c * b.threads;
-        const size_t regs = (size_t)((a_ctas * warps(a) + 3u) / 4u) * warp_regs(a.regs_per_thread) +
-                            (size_t)((c * warps(b) + 3u) / 4u) * warp_regs(b.regs_per_thread);
-        if (smem <= (size_t)smem_sm && threads <= (size_t)threads_sm && a_ctas + c <= (unsigned int)blocks_sm &&
-            regs <= part_regs)
-            return c;
-    }
-    return 0;
+    SmLimits sm;
+    sm.smem = (size_t)smem_sm;
+    sm.reserved = (size_t)reserved;
+    sm.regs = (size_t)regs_sm;
+    sm.threads = (size_t)threads_sm;
+    sm.blocks = (unsigned int)blocks_sm;
+    return ctas_beside(a, a_ctas, b, sm);
 }
 
 #define HRM_GUARD(...)                                           \

@@ -65,6 +65,17 @@ def test_spec_members_are_honoured_at_compile_time(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
 
 
+def test_co_residency_arithmetic_at_compile_time(tmp_path):
+    """tests/cpp/occupancy.cu: static checks of the CTAs-beside arithmetic that sizes the
+    serving session's resident share and solo photon kernel (B200 per-SM limits, registers per
+    sub-partition). nvcc cross-compiles it here; no kernel runs."""
+    src = os.path.join(ROOT, "tests", "cpp", "occupancy.cu")
+    r = subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I", os.path.join(ROOT, "include"), "-c", src, "-o", str(tmp_path / "occupancy.o")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 def test_bad_arguments_return_einval(hrm):
     L = hrm.lib()
     res = hrm.RunResult()
