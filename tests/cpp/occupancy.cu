@@ -2,7 +2,10 @@
 // per-SM limits: 233,472 B of shared memory with 1,024 B reserved per CTA, 65,536 registers
 // in four sub-partitions, 2,048 threads, 32 CTAs. The serving session sizes the resident
 // kernel's share and the solo photon kernel beside it with this function.
+#include "harmonize.h"
 #include "../../harmonize_b200/csrc/capi_internal.h"
+#include "../../harmonize_b200/csrc/specs/collatz.h"
+#include "../../harmonize_b200/csrc/specs/photon.h"
 
 using hrm_capi::ctas_beside;
 using hrm_capi::CtaFootprint;
@@ -11,10 +14,19 @@ using hrm_capi::SmLimits;
 constexpr SmLimits B200{233472u, 1024u, 65536u, 2048u, 32u};
 constexpr CtaFootprint NONE{0u, 0u, 0u};
 
-// Alone on an SM: the exec kernels of the tuned variants, as ncu reported them.
-constexpr CtaFootprint PHOTON_R4_T2_M11{80u, 64u, 18176u};  // 12 CTAs: shared memory and registers
-constexpr CtaFootprint COLLATZ_R3_T2_M14{72u, 64u, 6880u};  // 14 CTAs: registers (7 warps per sub-partition)
-constexpr CtaFootprint PHOTON_R3_T2_M14{72u, 64u, 14848u};  // 14 CTAs: shared memory and registers
+// Alone on an SM: the exec kernels of the tuned variants, with the registers ptxas gives them
+// under their launch bounds and the stash sizes of their program types (as ncu reported them).
+using hrm_capi::MinCtas;
+using PhotonR4T2M11 = AsyncProgram<MinCtas<hrm_specs::PhotonSpec<4, 2>, 11>>;
+using PhotonR3T2M14 = AsyncProgram<MinCtas<hrm_specs::PhotonSpec<3, 2>, 14>>;
+using CollatzR3T2M14 = AsyncProgram<MinCtas<hrm_specs::CollatzSpec<3, 2>, 14>>;
+static_assert(PhotonR4T2M11::SMEM_BYTES == 18176u && PhotonR3T2M14::SMEM_BYTES == 14848u &&
+                  CollatzR3T2M14::SMEM_BYTES == 6880u,
+              "stash bytes per CTA of 2 teams: photon R4 18,176, photon R3 14,848, Collatz R3 6,880");
+static_assert(PhotonR4T2M11::CTA_THREADS == 64u && PhotonR3T2M14::MIN_CTAS_PER_SM == 14u, "2 teams; launch bound");
+constexpr CtaFootprint PHOTON_R4_T2_M11{80u, 64u, PhotonR4T2M11::SMEM_BYTES};    // 12 CTAs: shared memory and registers
+constexpr CtaFootprint COLLATZ_R3_T2_M14{72u, 64u, CollatzR3T2M14::SMEM_BYTES};  // 14 CTAs: registers (7 warps per sub-partition)
+constexpr CtaFootprint PHOTON_R3_T2_M14{72u, 64u, PhotonR3T2M14::SMEM_BYTES};    // 14 CTAs: shared memory and registers
 static_assert(ctas_beside(NONE, 0u, PHOTON_R4_T2_M11, B200) == 12u, "photon R4/T2: 12 CTAs per SM");
 static_assert(ctas_beside(NONE, 0u, COLLATZ_R3_T2_M14, B200) == 14u, "Collatz R3/T2: 14 CTAs per SM");
 static_assert(ctas_beside(NONE, 0u, PHOTON_R3_T2_M14, B200) == 14u, "photon R3/T2: 14 CTAs per SM");
